@@ -1,0 +1,167 @@
+// Shared host/device infrastructure of the insem B200 backend: status
+// handling behind the C ABI, device buffers, launch checks and the
+// IEEE-ordered float helpers every kernel uses.
+//
+// Arithmetic contract: the reference's float build on x86-64 rounds every
+// product and sum separately (no FMA contraction; the INSEM_STRICT_FP build
+// is bit-identical to the default one there).  All kernels therefore build
+// their sums from __fmul_rn / __fadd_rn (never contracted), in the order the
+// reference writes them, and the library is compiled with -fmad=false so
+// that double arithmetic (Stacey solves, receivers, energy) is not
+// contracted either.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/insem_cuda.h"
+
+namespace insem_b200 {
+
+// ------------------------------------------------------------------ errors
+// Error carrying a C-ABI status code; thrown inside the library and turned
+// into a return code plus thread-local message at the boundary.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& msg) : std::runtime_error(msg), code(c) {}
+};
+
+void set_last_error(const std::string& msg);
+const char* last_error();
+
+#define INSEM_REQUIRE(cond, code, msg)                                          \
+  do {                                                                          \
+    if (!(cond)) throw ::insem_b200::Error((code), std::string(msg));           \
+  } while (0)
+
+#define CUDA_CHECK(expr)                                                        \
+  do {                                                                          \
+    cudaError_t err__ = (expr);                                                 \
+    if (err__ != cudaSuccess)                                                   \
+      throw ::insem_b200::Error(INSEM_CUDA_ERR_CUDA,                            \
+                                std::string(#expr) + ": " + cudaGetErrorString(err__)); \
+  } while (0)
+
+#define CUDA_LAUNCH_CHECK() CUDA_CHECK(cudaGetLastError())
+
+// Runs `fn` and converts exceptions to a status code (C-ABI wrapper).
+template <class Fn>
+int guarded(Fn&& fn) {
+  try {
+    fn();
+    set_last_error("");
+    return INSEM_CUDA_OK;
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_last_error("host memory allocation failed");
+    return INSEM_CUDA_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return INSEM_CUDA_ERR_INVALID;
+  }
+}
+
+// ------------------------------------------------------------ device memory
+// Owning device buffer.  Allocation failures report INSEM_CUDA_ERR_NOMEM.
+template <class T>
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  explicit DeviceBuffer(std::size_t n) { resize(n); }
+  ~DeviceBuffer() { release(); }
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept : p_(o.p_), n_(o.n_) { o.p_ = nullptr; o.n_ = 0; }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    if (this != &o) {
+      release();
+      p_ = o.p_;
+      n_ = o.n_;
+      o.p_ = nullptr;
+      o.n_ = 0;
+    }
+    return *this;
+  }
+  void resize(std::size_t n) {
+    release();
+    if (n == 0) return;
+    cudaError_t e = cudaMalloc(&p_, n * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      p_ = nullptr;
+      throw Error(INSEM_CUDA_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(T)) +
+                                            " bytes failed: " + cudaGetErrorString(e));
+    }
+    n_ = n;
+  }
+  void upload(const T* host, std::size_t n) {
+    resize(n);
+    if (n) CUDA_CHECK(cudaMemcpy(p_, host, n * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
+  void zero(cudaStream_t s = nullptr) {
+    if (n_) CUDA_CHECK(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
+  }
+  std::vector<T> download() const {
+    std::vector<T> out(n_);
+    if (n_) CUDA_CHECK(cudaMemcpy(out.data(), p_, n_ * sizeof(T), cudaMemcpyDeviceToHost));
+    return out;
+  }
+  T* get() { return p_; }
+  const T* get() const { return p_; }
+  std::size_t size() const { return n_; }
+  std::size_t bytes() const { return n_ * sizeof(T); }
+
+ private:
+  void release() {
+    if (p_) cudaFree(p_);
+    p_ = nullptr;
+    n_ = 0;
+  }
+  T* p_ = nullptr;
+  std::size_t n_ = 0;
+};
+
+// Copies a host array given by pointer and count (nullptr allowed when n == 0).
+template <class T>
+std::vector<T> host_vec(const T* p, std::size_t n) {
+  if (n == 0) return {};
+  INSEM_REQUIRE(p != nullptr, INSEM_CUDA_ERR_INVALID, "null array pointer for a non-empty array");
+  return std::vector<T>(p, p + n);
+}
+
+// Makes `device` current for the lifetime of the guard.
+class DeviceGuard {
+ public:
+  explicit DeviceGuard(int device) {
+    CUDA_CHECK(cudaGetDevice(&old_));
+    if (device != old_) CUDA_CHECK(cudaSetDevice(device));
+  }
+  ~DeviceGuard() { cudaSetDevice(old_); }
+
+ private:
+  int old_ = 0;
+};
+
+// ------------------------------------------------- IEEE-ordered arithmetic
+// Round-to-nearest operations that the compiler never fuses: sums and
+// products are evaluated exactly as the reference writes them.
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+
+inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+
+}  // namespace insem_b200

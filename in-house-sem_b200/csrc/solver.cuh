@@ -1,0 +1,114 @@
+// Device-resident solver state (the twin of solver::Solver).
+#pragma once
+
+#include <random>
+#include <vector>
+
+#include "device_data.cuh"
+#include "step_kernels.cuh"
+
+namespace insem_b200 {
+
+// One medium's fields and per-step arrays in HBM (solver::Domain, solver.hpp:25-66).
+struct DeviceDomainData {
+  int medium = 0, m = 0, ncomp = 1, ng = 0, npe = 0, n_elements = 0;
+  DeviceDofMap dofs;
+  std::vector<DeviceBlock> blocks;
+  bool any_axial = false;
+  std::vector<float> host_mass;
+  DeviceBuffer<float> mass, inv_mass;
+  int32_t n_abs = 0;
+  DeviceBuffer<int32_t> absorbing_points;
+  DeviceBuffer<float> absorbing_coef;
+  std::vector<int64_t> host_zero;   // Dirichlet and axis entries (component * ng + point)
+  DeviceBuffer<int64_t> zero_idx;
+  DeviceBuffer<float> u, v, a, f, f_local;
+
+  void upload(const insem_cuda_domain& d, const insem_cuda_basis& basis);
+};
+
+struct DomainSources {
+  int32_t n_points = 0;
+  DeviceBuffer<int32_t> points, offsets, source;
+  DeviceBuffer<float> coef;
+};
+
+struct TraceInfo {
+  int32_t first_col = 0;
+  int32_t ncomp = 0;
+};
+
+class Solver {
+ public:
+  // setup_only: dt may be 0 (the problem is used to estimate the stable time step).
+  Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool setup_only = false);
+  ~Solver();
+  Solver(const Solver&) = delete;
+  Solver& operator=(const Solver&) = delete;
+
+  void set_state(int32_t medium, const double* u, const double* v);
+  void advance(int32_t n);
+  int32_t n_samples() const;
+  int32_t n_energy() const;
+  void copy_trace(int32_t t, double* out);
+  void copy_state(int32_t di, double* u, double* v, double* a);
+  // f = -K u for a domain: gather-fused element kernels + CSR assemble.
+  void internal_forces(DeviceDomainData& d, const float* u_global, float* f_global);
+  // Power iteration for lambda_max(M^-1 K) (solver.cpp:583-667); returns 2/sqrt(lambda).
+  double stable_dt();
+
+  insem_cuda_options opts{};
+  int device = 0;
+  int ngll = 0;
+  double dt = 0.0;
+  int32_t n_steps = 0, step = 0, record_every = 1, energy_every = 0;
+  bool initialized = false;
+  double last_ms = 0.0;
+  cudaStream_t stream = nullptr;
+  std::vector<DeviceDomainData> domains;
+  std::vector<TraceInfo> traces;
+  DeviceBuffer<double> energy;  // [n_energy][3]
+
+ private:
+  void build_coupling(const insem_cuda_coupling& c);
+  void build_sources(const insem_cuda_problem& p);
+  void build_receivers(const insem_cuda_problem& p);
+  ReceiversDev receivers_view();
+  AllFields fields_view();
+  void domain_acceleration(int di, int pot_set, int force_energy, double h, int step_override);
+  void compute_acceleration(int force_energy, double h, int step_override);
+  void observers(int force_energy, int init);
+  void enqueue_step();
+  void initialize();
+  double reduce_partials();
+  void zero_constrained(DeviceDomainData& d, float* x);
+  void coupling_forces(int di);
+  double coupled_lambda_max(std::mt19937& rng);
+
+  DeviceBasis basis;
+  int solid = -1, fluid = -1;
+  // coupling
+  int32_t n_cpl = 0;
+  bool cpl_serial_fluid = false, cpl_serial_solid = false;
+  DeviceBuffer<int32_t> cpl_fluid, cpl_solid;
+  DeviceBuffer<float> cpl_cx, cpl_cz;
+  // sources
+  int32_t n_sources = 0, n_amp = 0;
+  DeviceBuffer<float> src_amp;
+  std::vector<DomainSources> src;
+  // receivers
+  int32_t n_receivers = 0, n_cols = 0, n_acoustic_rec = 0, max_samples = 0;
+  DeviceBuffer<int32_t> rec_offsets, rec_points, rec_domain, rec_acoustic;
+  DeviceBuffer<float> rec_value, rec_ddx, rec_ddz;
+  DeviceBuffer<double> rec_rho, rec_pv, trace_buf;
+  DeviceBuffer<RecordColumn> rec_cols;
+  // energy
+  DeviceBuffer<double> partial;
+  int n_pot_sets = 0;
+  // step state and graph
+  StepState* st = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+}  // namespace insem_b200

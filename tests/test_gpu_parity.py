@@ -1,0 +1,115 @@
+"""CUDA path vs the reference's own outputs (golden fixtures made from the
+reference build): per-block force vectors, gather, assemble and internal
+forces bit for bit; full-run receiver traces, sample times and final fields
+bit for bit; energy samples to 1e-9 relative (FP64 reductions in a different
+order); the stable time step to 1e-6 relative."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import BLK_CASES, RUN_CASES, golden
+import golden_io as G
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    return np.ascontiguousarray(np.asarray(a, np.float32)).view(np.uint32)
+
+
+@pytest.mark.parametrize("case", RUN_CASES + BLK_CASES)
+def test_block_forces_bitwise(pkg, case):
+    from insem_b200 import kernels
+
+    z = golden(case)
+    n = 0
+    for prefix, prob in G.sub_problems(pkg, z):
+        for di, d in enumerate(prob.domains):
+            u = G.block_input(d, di)
+            for bi in range(len(d.blocks)):
+                f = kernels.block_forces(prob, di, bi, u)
+                gold = z[f"{prefix}gold.d{di}.b{bi}.f_local"]
+                assert np.array_equal(bits(f), bits(gold)), f"{case} {prefix} d{di} b{bi}"
+                n += 1
+    assert n > 0
+
+
+@pytest.mark.parametrize("case", RUN_CASES + BLK_CASES)
+def test_gather_assemble_bitwise(pkg, case):
+    import torch
+    from insem_b200 import kernels
+
+    z = golden(case)
+    for prefix, prob in G.sub_problems(pkg, z):
+        for di, d in enumerate(prob.domains):
+            k = kernels.DofMapKernel(prob.ngll, d)
+            g = torch.from_numpy(G.gather_input(d, di)).cuda()
+            loc = torch.empty(d.ncomp * d.l2g.size, dtype=torch.float32, device="cuda")
+            k.gather_device(d.ncomp, g.data_ptr(), loc.data_ptr())
+            fl = torch.from_numpy(G.assemble_input(d, di)).cuda()
+            glob = torch.empty(d.ncomp * d.n_global, dtype=torch.float32, device="cuda")
+            k.assemble_device(d.ncomp, fl.data_ptr(), glob.data_ptr())
+            torch.cuda.synchronize()
+            assert np.array_equal(bits(loc.cpu().numpy()), bits(z[f"{prefix}gold.d{di}.gather"]))
+            assert np.array_equal(bits(glob.cpu().numpy()), bits(z[f"{prefix}gold.d{di}.assemble"]))
+            k.close()
+
+
+@pytest.mark.parametrize("case", RUN_CASES + BLK_CASES)
+def test_internal_forces_bitwise(pkg, case):
+    z = golden(case)
+    for prefix, prob in G.sub_problems(pkg, z):
+        with pkg.Solver(prob) as s:
+            for di, d in enumerate(prob.domains):
+                f = s.internal_forces(di, G.forces_input(d, di))
+                assert np.array_equal(bits(f), bits(z[f"{prefix}gold.d{di}.internal_forces"]))
+
+
+def run_case(pkg, z, **opts):
+    prob = pkg.ProblemData.from_npz(z)
+    s = pkg.Solver(prob, **opts)
+    for di, d in enumerate(prob.domains):
+        if f"init.d{di}.u" in z.files and (np.any(z[f"init.d{di}.u"]) or np.any(z[f"init.d{di}.v"])):
+            s.set_state(prob.media[di], z[f"init.d{di}.u"].astype(np.float64), z[f"init.d{di}.v"].astype(np.float64))
+    s.advance(int(z["run.advance_first"]))
+    s.run()
+    return prob, s
+
+
+@pytest.mark.parametrize("graphs", [True, False])
+@pytest.mark.parametrize("case", RUN_CASES)
+def test_run_bitwise(pkg, case, graphs):
+    z = golden(case)
+    prob, s = run_case(pkg, z, use_graphs=graphs)
+    with s:
+        assert s.step == prob.n_steps
+        assert np.array_equal(s.times, z["run.times"])
+        for name, q in prob.trace_list():
+            gold = z[f"run.trace.{name}.{q}"]
+            got = s.trace(name, q)
+            assert got.shape == gold.shape
+            assert np.array_equal(got, gold), f"{case} {name}/{q}: rel L2 {G.rel_l2(got, gold):.3e}"
+        for di in range(len(prob.domains)):
+            u, v, a = s.state(prob.media[di])
+            for key, arr in (("u", u), ("v", v), ("a", a)):
+                gold = z[f"run.d{di}.{key}"].astype(np.float64).reshape(arr.shape)
+                assert np.array_equal(arr, gold), f"{case} d{di} {key}"
+        e = s.energy
+        ge = z["run.energy"]
+        assert e.shape == ge.shape
+        if ge.size:
+            assert np.array_equal(e[:, 0], ge[:, 0])
+            scale = np.abs(ge[:, 1:]).max()
+            assert np.abs(e[:, 1:] - ge[:, 1:]).max() <= 1e-9 * scale
+
+
+@pytest.mark.parametrize("case", ["c1", "bh0", "lay", "box"])
+def test_stable_dt(pkg, case):
+    from insem_b200.solver import estimate_stable_dt
+
+    z = golden(case)
+    prob = pkg.ProblemData.from_npz(z)
+    dt = estimate_stable_dt(prob)
+    assert abs(dt - prob.stable_dt) <= 1e-6 * prob.stable_dt, (dt, prob.stable_dt)
