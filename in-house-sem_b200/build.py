@@ -22,6 +22,7 @@ REPO = PKG.parent
 CSRC = PKG / "csrc"
 OBJ = PKG / "_build" / "obj"
 LIB = PKG / "lib" / "libinsem_cuda.so"
+CASES_LIB = PKG / "lib" / "libinsem_cases.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -66,8 +67,25 @@ def compile_unit(src: Path, extra: list[str], obj: Path, verbose: bool, force: b
     return res.stderr if verbose else f"built {obj.name}"
 
 
+def build_cases(force: bool = False) -> Path:
+    """Host-only case-setup library (csrc/host), compiled with the system C++ compiler."""
+    src = CSRC / "host" / "cases.cpp"
+    hdr = CSRC / "host" / "insem_cases.h"
+    if force or not CASES_LIB.exists() or CASES_LIB.stat().st_mtime < max(src.stat().st_mtime, hdr.stat().st_mtime):
+        CASES_LIB.parent.mkdir(parents=True, exist_ok=True)
+        cxx = shutil.which("g++") or "c++"
+        tmp = CASES_LIB.with_suffix(".so.tmp")
+        cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", str(src), "-o", str(tmp)]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"case library build failed:\n{res.stderr[-6000:]}")
+        tmp.replace(CASES_LIB)
+    return CASES_LIB
+
+
 def build(jobs: int | None = None, verbose: bool = False, force: bool = False) -> Path:
     jobs = jobs or max(1, min(16, os.cpu_count() or 1))
+    build_cases(force)
     todo = units()
     with ThreadPoolExecutor(max_workers=jobs) as ex:
         logs = list(ex.map(lambda u: compile_unit(*u, verbose, force), todo))

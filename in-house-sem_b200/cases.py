@@ -1,0 +1,440 @@
+"""Model descriptions and the benchmark / serving workloads, built natively.
+
+``Model`` holds what the reference's ``Simulation`` describes (mesh,
+discretisation, materials, boundaries, sources, receivers, time settings,
+cpp/include/insem/sim/simulation.hpp:56-124); ``build`` runs the native
+setup (csrc/host/cases.cpp) and the device power iteration for the stable
+time step, and returns the ``ProblemData`` the solver takes.
+
+The mesh templates follow the node-lattice, cell-ordering and boundary-tag
+conventions of the reference's python/insem/mesh/templates.py (BOTTOM 1,
+RIGHT 2, TOP 3, LEFT 4; Quad9 cells honour curved interfaces).
+
+Workloads (seeded; shapes and value ranges as the benchmark configurations
+state them):
+  config1   32x32 acoustic rectangle, order 4, Stacey, Ricker 400 Hz (4 ms)
+  config2   cased borehole m = 0, order 4, f_max 7.5 kHz, AMR (5 ms)
+  config3   1024x1024 coupled water / 8 curved elastic layers, order 5 (2000 steps)
+  config4   256 boreholes, m = 0 / 1, order 4-6, 1-6 beds, casing in 30 %
+  serving   Poisson mix of Cartesian and borehole requests
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence, Tuple, Union
+
+import numpy as np
+
+from . import native as N
+from .problem import ProblemData
+
+BOTTOM, RIGHT, TOP, LEFT = 1, 2, 3, 4
+MEDIUM = {"acoustic": 0, "elastic": 1}
+BC = {"free": 0, "rigid": 1, "absorbing": 2}
+SOURCE_KIND = {"force": 0, "moment_tensor": 1, "monopole": 2, "dipole": 3}
+STF_KIND = {"ricker": 0, "gaussian": 1, "gaussian_derivative": 2}
+
+
+# ------------------------------------------------------------------ meshes
+@dataclass
+class MacroMesh:
+    quad9: bool
+    axisymmetric: bool
+    nodes: np.ndarray      # (n_nodes, 2)
+    cells: np.ndarray      # (n_cells, 4 or 9)
+    region: np.ndarray     # (n_cells,)
+    boundary: np.ndarray   # (n_faces, 3) cell, face, tag
+
+
+def _lattice(breaks: np.ndarray, quadratic: bool) -> np.ndarray:
+    if not quadratic:
+        return breaks
+    out = np.empty(2 * breaks.size - 1)
+    out[0::2] = breaks
+    out[1::2] = 0.5 * (breaks[:-1] + breaks[1:])
+    return out
+
+
+def _structured(xl: np.ndarray, zl: np.ndarray, quadratic: bool, region: np.ndarray, axisym: bool) -> MacroMesh:
+    """Cells row by row (x fastest) over a node lattice: xl (mx,), zl (mz, mx)."""
+    step = 2 if quadratic else 1
+    mx = xl.size
+    ncx, ncz = (mx - 1) // step, (zl.shape[0] - 1) // step
+    if np.any(np.diff(zl, axis=0) <= 0):
+        raise ValueError("layer interfaces must increase in z at every x")
+    nodes = np.column_stack([np.broadcast_to(xl, zl.shape).ravel(), zl.ravel()])
+    jj, ii = np.meshgrid(np.arange(ncz), np.arange(ncx), indexing="ij")
+    a, b = (step * ii).ravel(), (step * jj).ravel()
+
+    def node(i, j):
+        return i + mx * j
+
+    if quadratic:
+        cells = np.stack([node(a, b), node(a + 2, b), node(a + 2, b + 2), node(a, b + 2), node(a + 1, b),
+                          node(a + 2, b + 1), node(a + 1, b + 2), node(a, b + 1), node(a + 1, b + 1)], axis=1)
+    else:
+        cells = np.stack([node(a, b), node(a + 1, b), node(a + 1, b + 1), node(a, b + 1)], axis=1)
+    c = np.arange(ncx * ncz)
+    i, j = c % ncx, c // ncx
+    faces = []
+    for cond, face, tag in ((j == 0, 0, BOTTOM), (i == ncx - 1, 1, RIGHT), (j == ncz - 1, 2, TOP), (i == 0, 3, LEFT)):
+        sel = c[cond]
+        faces.append(np.stack([sel, np.full(sel.size, face), np.full(sel.size, tag), sel * 4 + face], axis=1))
+    f = np.concatenate(faces)
+    f = f[np.argsort(f[:, 3], kind="stable")][:, :3]  # per cell in face order, as the template loops
+    return MacroMesh(quadratic, axisym, np.ascontiguousarray(nodes, float), np.ascontiguousarray(cells, np.int32),
+                     np.ascontiguousarray(region, np.int32), np.ascontiguousarray(f, np.int32))
+
+
+def _axis(spec, n: Optional[int]) -> np.ndarray:
+    v = np.asarray(spec, float)
+    return v if n is None else np.linspace(v[0], v[1], n + 1)
+
+
+def rectangle(x, z, nx=None, nz=None, material: Union[int, Sequence[int], Callable] = 0, quadratic=False,
+              coords="cartesian") -> MacroMesh:
+    xs, zs = _axis(x, nx), _axis(z, nz)
+    ncx, ncz = xs.size - 1, zs.size - 1
+    xl = _lattice(xs, quadratic)
+    zl = np.repeat(_lattice(zs, quadratic)[:, None], xl.size, axis=1)
+    if callable(material):
+        xc, zc = 0.5 * (xs[:-1] + xs[1:]), 0.5 * (zs[:-1] + zs[1:])
+        mat = np.array([material(xc[i], zc[j]) for j in range(ncz) for i in range(ncx)], np.int32)
+    else:
+        mat = np.broadcast_to(np.asarray(material, np.int32), (ncx * ncz,)).copy()
+    return _structured(xl, zl, quadratic, mat, coords == "axisymmetric")
+
+
+def layered(x, interfaces, nz, regions, nx=None, quadratic=False, coords="cartesian") -> MacroMesh:
+    """Layers between K + 1 interfaces (constants or callables z(x)), bottom to top."""
+    xs = _axis(x, nx)
+    k = len(interfaces) - 1
+    counts = [int(nz)] * k if np.isscalar(nz) else [int(v) for v in nz]
+    xl = _lattice(xs, quadratic)
+    levels = [np.broadcast_to(np.asarray(i(xl) if callable(i) else float(i), float), xl.shape).astype(float)
+              for i in interfaces]
+    step = 2 if quadratic else 1
+    rows = [levels[0]]
+    for layer in range(k):
+        n_rows = step * counts[layer]
+        for r in range(1, n_rows + 1):
+            t = r / n_rows
+            rows.append((1.0 - t) * levels[layer] + t * levels[layer + 1])
+    zl = np.vstack(rows)
+    ncx = xs.size - 1
+    mat = np.concatenate([np.full(ncx * counts[layer], regions[layer], np.int32) for layer in range(k)])
+    return _structured(xl, zl, quadratic, mat, coords == "axisymmetric")
+
+
+def _graded(r0, r1, first, growth, max_size) -> List[float]:
+    out, r, size = [r0], r0, first
+    while r1 - r > 1e-12 * max(1.0, abs(r1)):
+        size = min(size, max_size)
+        if r1 - r <= 1.5 * size:
+            out.append(r1)
+            break
+        r += size
+        out.append(r)
+        size *= growth
+    return out
+
+
+@dataclass
+class Borehole:
+    mesh: MacroMesh
+    regions: Dict[str, int]
+    boundaries: Dict[str, int]
+
+
+def borehole(z, annuli, formation_radius, beds=(), dz=0.05, dr=None, growth=1.3, fluid_cells=2,
+             quadratic=False) -> Borehole:
+    """Axisymmetric borehole: annuli around the axis, graded formation split into beds."""
+    z0, z1 = float(z[0]), float(z[1])
+    radii = [float(r) for _, r in annuli]
+    beds = list(beds) or [(z0, "formation")]
+    dr = 4 * dz if dr is None else dr
+    r_breaks = list(np.linspace(0.0, radii[0], fluid_cells + 1))
+    last = radii[0] / fluid_cells
+    for inner, outer in zip(radii, radii[1:]):
+        n = max(1, int(np.ceil((outer - inner) / dz - 1e-9)))
+        r_breaks += list(np.linspace(inner, outer, n + 1)[1:])
+        last = (outer - inner) / n
+    r_breaks += _graded(radii[-1], formation_radius, min(last * growth, dr), growth, dr)[1:]
+    tops = [b[0] for b in beds[1:]] + [z1]
+    z_breaks = [z0]
+    for bottom, top in zip([b[0] for b in beds], tops):
+        n = max(1, int(np.ceil((top - bottom) / dz - 1e-9)))
+        z_breaks += list(np.linspace(bottom, top, n + 1)[1:])
+    names: Dict[str, int] = {}
+    for name in [a for a, _ in annuli] + [b for _, b in beds]:
+        names.setdefault(name, len(names) + 1)
+    bottoms = np.array([b[0] for b in beds])
+
+    def region(rc, zc):
+        for name, outer in annuli:
+            if rc < outer:
+                return names[name]
+        return names[beds[int(np.searchsorted(bottoms, zc, side="right")) - 1][1]]
+
+    m = rectangle(r_breaks, z_breaks, material=region, quadratic=quadratic, coords="axisymmetric")
+    return Borehole(m, names, {"bottom": BOTTOM, "outer": RIGHT, "top": TOP, "axis": LEFT})
+
+
+# ------------------------------------------------------------------ model
+@dataclass
+class Material:
+    medium: str
+    vp: float
+    vs: float
+    rho: float
+
+    @staticmethod
+    def acoustic(vp, rho):
+        return Material("acoustic", vp, 0.0, rho)
+
+    @staticmethod
+    def elastic(vp, vs, rho):
+        return Material("elastic", vp, vs, rho)
+
+
+@dataclass
+class Source:
+    kind: str
+    x: float
+    z: float
+    components: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    stf: Tuple[str, float, float, float] = ("ricker", 1.0, -1.0, 1.0)  # kind, f0, t0 (-1: 1.2/f0), amplitude
+
+
+def ricker(f0, t0=-1.0, amplitude=1.0):
+    return ("ricker", f0, t0, amplitude)
+
+
+@dataclass
+class Receiver:
+    name: str
+    x: float
+    z: float
+    quantities: List[str]
+    medium: str = ""
+
+
+@dataclass
+class Model:
+    mesh: MacroMesh
+    order: int = 4
+    uniform_level: int = 0
+    f_max: float = 0.0
+    points_per_wavelength: float = 5.0
+    max_level: int = 12
+    regions: List[Tuple[float, float, float, float, int]] = field(default_factory=list)
+    azimuthal_order: int = 0
+    materials: Dict[int, Material] = field(default_factory=dict)
+    boundaries: Dict[int, str] = field(default_factory=dict)
+    sources: List[Source] = field(default_factory=list)
+    receivers: List[Receiver] = field(default_factory=list)
+    duration: float = 0.0
+    n_steps: int = 0
+    dt: float = 0.0
+    safety: float = 0.8
+    record_every: int = 1
+    energy_every: int = 0
+
+
+_cases_lib = None
+
+
+def cases_lib() -> C.CDLL:
+    global _cases_lib
+    if _cases_lib is None:
+        path = N.PKG / "lib" / "libinsem_cases.so"
+        if not path.exists():
+            raise N.InsemError(N.ERR_INVALID, f"case setup library missing: {path} (run build.py)")
+        L = C.CDLL(str(path))
+        L.insem_case_build.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+        L.insem_case_build.restype = C.c_int
+        L.insem_case_n_arrays.argtypes = [C.c_void_p]
+        L.insem_case_n_arrays.restype = C.c_int32
+        L.insem_case_array_at.argtypes = [C.c_void_p, C.c_int32]
+        L.insem_case_array_at.restype = C.c_void_p
+        L.insem_case_free.argtypes = [C.c_void_p]
+        L.insem_case_last_error.restype = C.c_char_p
+        _cases_lib = L
+    return _cases_lib
+
+
+class _Desc(C.Structure):
+    _fields_ = [("quad9", C.c_int32), ("axisymmetric", C.c_int32), ("n_nodes", C.c_int32), ("nodes", C.c_void_p),
+                ("n_cells", C.c_int32), ("cells", C.c_void_p), ("cell_region", C.c_void_p),
+                ("n_boundary", C.c_int32), ("boundary", C.c_void_p), ("order", C.c_int32),
+                ("uniform_level", C.c_int32), ("f_max", C.c_double), ("points_per_wavelength", C.c_double),
+                ("max_level", C.c_int32), ("n_regions", C.c_int32), ("regions", C.c_void_p),
+                ("azimuthal_order", C.c_int32), ("n_materials", C.c_int32), ("material_region", C.c_void_p),
+                ("material_medium", C.c_void_p), ("material_vp", C.c_void_p), ("material_vs", C.c_void_p),
+                ("material_rho", C.c_void_p), ("n_bc", C.c_int32), ("bc_tag", C.c_void_p), ("bc_type", C.c_void_p),
+                ("n_sources", C.c_int32), ("source_kind", C.c_void_p), ("source_position", C.c_void_p),
+                ("source_components", C.c_void_p), ("stf_kind", C.c_void_p), ("stf_params", C.c_void_p),
+                ("n_receivers", C.c_int32), ("receiver_position", C.c_void_p), ("receiver_medium", C.c_void_p),
+                ("receiver_qoffsets", C.c_void_p), ("receiver_quantities", C.c_void_p),
+                ("record_every", C.c_int32), ("energy_every", C.c_int32)]
+
+
+class _CArray(C.Structure):
+    _fields_ = [("key", C.c_char_p), ("dtype", C.c_int32), ("n", C.c_int64), ("data", C.c_void_p)]
+
+
+_DT = {0: np.float32, 1: np.float64, 2: np.int32, 3: np.uint8}
+
+
+def setup_arrays(model: Model) -> Dict[str, np.ndarray]:
+    """Runs the native setup; returns the flat problem layout (dt not set)."""
+    keep = []
+
+    def arr(a, dtype):
+        a = np.ascontiguousarray(np.asarray(a, dtype))
+        keep.append(a)
+        return a.ctypes.data if a.size else None
+
+    m = model.mesh
+    d = _Desc()
+    d.quad9, d.axisymmetric = int(m.quad9), int(m.axisymmetric)
+    d.n_nodes, d.nodes = m.nodes.shape[0], arr(m.nodes, np.float64)
+    d.n_cells, d.cells, d.cell_region = m.cells.shape[0], arr(m.cells, np.int32), arr(m.region, np.int32)
+    d.n_boundary, d.boundary = m.boundary.shape[0], arr(m.boundary, np.int32)
+    d.order, d.uniform_level, d.f_max = model.order, model.uniform_level, model.f_max
+    d.points_per_wavelength, d.max_level = model.points_per_wavelength, model.max_level
+    d.n_regions, d.regions = len(model.regions), arr(np.asarray(model.regions, float).reshape(-1, 5), np.float64)
+    d.azimuthal_order = model.azimuthal_order
+    mats = sorted(model.materials.items())
+    d.n_materials = len(mats)
+    d.material_region = arr([r for r, _ in mats], np.int32)
+    d.material_medium = arr([MEDIUM[x.medium] for _, x in mats], np.int32)
+    d.material_vp = arr([x.vp for _, x in mats], np.float64)
+    d.material_vs = arr([x.vs for _, x in mats], np.float64)
+    d.material_rho = arr([x.rho for _, x in mats], np.float64)
+    bcs = sorted(model.boundaries.items())
+    d.n_bc, d.bc_tag, d.bc_type = len(bcs), arr([t for t, _ in bcs], np.int32), arr([BC[b] for _, b in bcs], np.int32)
+    src = model.sources
+    d.n_sources = len(src)
+    d.source_kind = arr([SOURCE_KIND[s.kind] for s in src], np.int32)
+    d.source_position = arr([[s.x, s.z] for s in src], np.float64)
+    d.source_components = arr([list(s.components) for s in src], np.float64)
+    d.stf_kind = arr([STF_KIND[s.stf[0]] for s in src], np.int32)
+    d.stf_params = arr([[s.stf[1], s.stf[2] if s.stf[2] >= 0 else 1.2 / s.stf[1], s.stf[3]] for s in src], np.float64)
+    rec = model.receivers
+    d.n_receivers = len(rec)
+    d.receiver_position = arr([[r.x, r.z] for r in rec], np.float64)
+    d.receiver_medium = arr([MEDIUM.get(r.medium, -1) for r in rec], np.int32)
+    qoff = np.cumsum([0] + [len(r.quantities) for r in rec])
+    d.receiver_qoffsets = arr(qoff, np.int32)
+    d.receiver_quantities = arr([N.QUANTITIES[q] for r in rec for q in r.quantities], np.int32)
+    d.record_every, d.energy_every = model.record_every, model.energy_every
+
+    L = cases_lib()
+    out = C.c_void_p()
+    if L.insem_case_build(C.byref(d), C.byref(out)) != 0:
+        raise N.InsemError(N.ERR_INVALID, L.insem_case_last_error().decode())
+    try:
+        res = {}
+        for i in range(L.insem_case_n_arrays(out)):
+            a = _CArray.from_address(L.insem_case_array_at(out, i))
+            dt = _DT[a.dtype]
+            if a.n:
+                buf = (C.c_char * (a.n * np.dtype(dt).itemsize)).from_address(a.data)
+                res[a.key.decode()] = np.frombuffer(buf, dtype=dt).copy()
+            else:
+                res[a.key.decode()] = np.zeros(0, dt)
+    finally:
+        L.insem_case_free(out)
+    names = {}
+    for ri, r in enumerate(rec):
+        res[f"problem.receivers.{ri}.name"] = np.asarray(r.name)
+        res[f"problem.receivers.{ri}.quantities"] = np.asarray(r.quantities, dtype="U32")
+    for si in range(len(src)):
+        res[f"problem.sources.{si}.stf.samples"] = np.zeros(0)
+        res[f"problem.sources.{si}.stf.sample_dt"] = np.asarray(0.0)
+    return res
+
+
+def build(model: Model, device: int = 0, stable_dt: Optional[float] = None) -> ProblemData:
+    """Native setup, then dt = safety x the device power-iteration estimate (or model.dt)."""
+    from .solver import estimate_stable_dt
+
+    arrays = setup_arrays(model)
+    arrays["problem.dt"] = np.asarray(1.0)
+    arrays["problem.n_steps"] = np.asarray(0)
+    arrays["problem.stable_dt"] = np.asarray(0.0)
+    prob = ProblemData.from_npz(arrays)
+    sdt = stable_dt if stable_dt is not None else estimate_stable_dt(prob, device)
+    prob.stable_dt = sdt
+    if model.dt > 0.0:
+        if model.dt > sdt:
+            raise N.InsemError(N.ERR_INVALID, f"time step {model.dt} s exceeds the stability limit {sdt} s")
+        prob.dt = model.dt
+    else:
+        prob.dt = model.safety * sdt
+    if model.n_steps > 0:
+        prob.n_steps = model.n_steps
+    elif model.duration > 0.0:
+        prob.n_steps = int(np.ceil(model.duration / prob.dt - 1e-9))
+    return prob
+
+
+# --------------------------------------------------------------- workloads
+MUD = Material.acoustic(1500.0, 1000.0)
+STEEL = Material.elastic(5900.0, 3200.0, 7850.0)
+CEMENT = Material.elastic(3000.0, 1600.0, 1900.0)
+FAST = Material.elastic(4000.0, 2300.0, 2400.0)
+
+
+def config1() -> Model:
+    m = rectangle((-4.0, 4.0), (-4.0, 4.0), nx=32, nz=32)
+    return Model(m, order=4, materials={0: Material.acoustic(1500.0, 1000.0)},
+                 boundaries={t: "absorbing" for t in (BOTTOM, RIGHT, TOP, LEFT)},
+                 sources=[Source("monopole", 0.0, 0.0, stf=ricker(400.0))],
+                 receivers=[Receiver("h1", 1.5, 0.0, ["pressure"])], duration=4e-3)
+
+
+def config2(z=(-1.5, 4.5), formation_radius=4.0) -> Model:
+    b = borehole(z, [("mud", 0.1), ("casing", 0.11), ("cement", 0.14)], formation_radius=formation_radius, dz=0.08)
+    mats = {b.regions["mud"]: MUD, b.regions["casing"]: STEEL, b.regions["cement"]: CEMENT,
+            b.regions["formation"]: FAST}
+    recs = [Receiver(f"r{i}", 0.05, 2.0 + 0.15 * i, ["pressure"]) for i in range(13)]
+    return Model(b.mesh, order=4, f_max=7500.0, materials=mats,
+                 boundaries={b.boundaries[n]: "absorbing" for n in ("bottom", "outer", "top")},
+                 sources=[Source("monopole", 0.0, 0.0, stf=ricker(8000.0))], receivers=recs, duration=5e-3)
+
+
+def config3(nx: int = 1024, n_steps: int = 2000, seed: int = 3, n_receivers: int = 512) -> Model:
+    """Water (60 m, 154/1024 of the rows) over 8 elastic layers with sinusoidal
+    interfaces (amplitude U(2, 6) m, wavelength U(80, 200) m), 400 m wide, order 5,
+    Quad9 cells; force source at (200, -20) Ricker 30 Hz; velocity receivers on
+    the seafloor; Stacey on sides and bottom, free surface on top.  nx = 1024 is
+    the benchmark size; rows scale with nx."""
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(2.0, 6.0, 7)
+    lam = rng.uniform(80.0, 200.0, 7)
+    vp = rng.uniform(2000.0, 5500.0, 8)
+    vs = vp * rng.uniform(0.45, 0.6, 8)
+    rho = rng.uniform(2000.0, 2700.0, 8)
+    zk = -340.0 + 340.0 * np.arange(1, 8) / 8.0
+    interfaces: list = [-340.0]
+    for k in range(7):
+        interfaces.append(lambda x, z0=zk[k], a=amp[k], l=lam[k]: z0 + a * np.sin(2.0 * np.pi * x / l))
+    interfaces += [0.0, 60.0]
+    rows_water = round(154 * nx / 1024)
+    rows_el = nx - rows_water
+    counts = [rows_el // 8 + (1 if k < rows_el % 8 else 0) for k in range(8)] + [rows_water]
+    regions = list(range(1, 9)) + [0]
+    m = layered((0.0, 400.0), interfaces, counts, regions, nx=nx, quadratic=True)
+    mats = {0: Material.acoustic(1500.0, 1000.0)}
+    for k in range(8):
+        mats[k + 1] = Material.elastic(float(vp[k]), float(vs[k]), float(rho[k]))
+    recs = [Receiver(f"sf{i}", float(x), -0.5, ["velocity"], "elastic")
+            for i, x in enumerate(np.linspace(1.0, 399.0, n_receivers))]
+    return Model(m, order=5, materials=mats,
+                 boundaries={BOTTOM: "absorbing", LEFT: "absorbing", RIGHT: "absorbing", TOP: "free"},
+                 sources=[Source("force", 200.0, -20.0, (0.0, 1.0, 0.0), ricker(30.0))], receivers=recs,
+                 n_steps=n_steps)
