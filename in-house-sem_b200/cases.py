@@ -290,6 +290,34 @@ _DT = {0: np.float32, 1: np.float64, 2: np.int32, 3: np.uint8}
 
 def setup_arrays(model: Model) -> Dict[str, np.ndarray]:
     """Runs the native setup; returns the flat problem layout (dt not set)."""
+    d, keep = describe(model)
+    L = cases_lib()
+    out = C.c_void_p()
+    if L.insem_case_build(C.byref(d), C.byref(out)) != 0:
+        raise N.InsemError(N.ERR_INVALID, L.insem_case_last_error().decode())
+    try:
+        res = {}
+        for i in range(L.insem_case_n_arrays(out)):
+            a = _CArray.from_address(L.insem_case_array_at(out, i))
+            dt = _DT[a.dtype]
+            if a.n:
+                buf = (C.c_char * (a.n * np.dtype(dt).itemsize)).from_address(a.data)
+                res[a.key.decode()] = np.frombuffer(buf, dtype=dt).copy()
+            else:
+                res[a.key.decode()] = np.zeros(0, dt)
+    finally:
+        L.insem_case_free(out)
+    for ri, r in enumerate(model.receivers):
+        res[f"problem.receivers.{ri}.name"] = np.asarray(r.name)
+        res[f"problem.receivers.{ri}.quantities"] = np.asarray(r.quantities, dtype="U32")
+    for si in range(len(model.sources)):
+        res[f"problem.sources.{si}.stf.samples"] = np.zeros(0)
+        res[f"problem.sources.{si}.stf.sample_dt"] = np.asarray(0.0)
+    return res
+
+
+def describe(model: Model):
+    """The model as an ``insem_case_desc`` struct, plus the arrays it points into."""
     keep = []
 
     def arr(a, dtype):
@@ -331,31 +359,7 @@ def setup_arrays(model: Model) -> Dict[str, np.ndarray]:
     d.receiver_qoffsets = arr(qoff, np.int32)
     d.receiver_quantities = arr([N.QUANTITIES[q] for r in rec for q in r.quantities], np.int32)
     d.record_every, d.energy_every = model.record_every, model.energy_every
-
-    L = cases_lib()
-    out = C.c_void_p()
-    if L.insem_case_build(C.byref(d), C.byref(out)) != 0:
-        raise N.InsemError(N.ERR_INVALID, L.insem_case_last_error().decode())
-    try:
-        res = {}
-        for i in range(L.insem_case_n_arrays(out)):
-            a = _CArray.from_address(L.insem_case_array_at(out, i))
-            dt = _DT[a.dtype]
-            if a.n:
-                buf = (C.c_char * (a.n * np.dtype(dt).itemsize)).from_address(a.data)
-                res[a.key.decode()] = np.frombuffer(buf, dtype=dt).copy()
-            else:
-                res[a.key.decode()] = np.zeros(0, dt)
-    finally:
-        L.insem_case_free(out)
-    names = {}
-    for ri, r in enumerate(rec):
-        res[f"problem.receivers.{ri}.name"] = np.asarray(r.name)
-        res[f"problem.receivers.{ri}.quantities"] = np.asarray(r.quantities, dtype="U32")
-    for si in range(len(src)):
-        res[f"problem.sources.{si}.stf.samples"] = np.zeros(0)
-        res[f"problem.sources.{si}.stf.sample_dt"] = np.asarray(0.0)
-    return res
+    return d, keep
 
 
 def build(model: Model, device: int = 0, stable_dt: Optional[float] = None) -> ProblemData:

@@ -568,20 +568,7 @@ void Solver::advance(int32_t n) {
   const int32_t todo = std::min<int32_t>(n, n_steps - step);
   if (todo > 0) {
     if (opts.use_graphs) {
-      if (!graph_exec) {
-        cudaGraph_t g;
-        CUDA_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        try {
-          enqueue_step();
-        } catch (...) {
-          cudaStreamEndCapture(stream, &g);
-          if (g) cudaGraphDestroy(g);
-          throw;
-        }
-        CUDA_CHECK(cudaStreamEndCapture(stream, &g));
-        CUDA_CHECK(cudaGraphInstantiate(&graph_exec, g, 0));
-        CUDA_CHECK(cudaGraphDestroy(g));
-      }
+      ensure_graph();
       for (int32_t s = 0; s < todo; ++s) CUDA_CHECK(cudaGraphLaunch(graph_exec, stream));
     } else {
       for (int32_t s = 0; s < todo; ++s) enqueue_step();
@@ -605,6 +592,66 @@ void Solver::advance(int32_t n) {
     CUDA_CHECK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
     INSEM_REQUIRE(!hs.nonfinite, INSEM_CUDA_ERR_NONFINITE, "the solution contains NaN or Inf (unstable time step?)");
   }
+}
+
+// Captures one step into a CUDA graph (once) and counts its kernel nodes.
+void Solver::ensure_graph() {
+  if (graph_exec) return;
+  cudaGraph_t g = nullptr;
+  CUDA_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    enqueue_step();
+  } catch (...) {
+    cudaStreamEndCapture(stream, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  CUDA_CHECK(cudaStreamEndCapture(stream, &g));
+  std::size_t n_nodes = 0;
+  CUDA_CHECK(cudaGraphGetNodes(g, nullptr, &n_nodes));
+  std::vector<cudaGraphNode_t> nodes(n_nodes);
+  if (n_nodes) CUDA_CHECK(cudaGraphGetNodes(g, nodes.data(), &n_nodes));
+  kernels_per_step = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    CUDA_CHECK(cudaGraphNodeGetType(nd, &t));
+    if (t == cudaGraphNodeTypeKernel) ++kernels_per_step;
+  }
+  CUDA_CHECK(cudaGraphInstantiate(&graph_exec, g, 0));
+  CUDA_CHECK(cudaGraphDestroy(g));
+}
+
+// Per step: source amplitudes in (H2D), the step's graph, the record row out (D2H).
+void Solver::advance_streamed(int32_t n, const float* amp_in, double* rows_out, int32_t* n_rows) {
+  DeviceGuard dg(device);
+  INSEM_REQUIRE(n >= 0 && n_rows, INSEM_CUDA_ERR_INVALID, "invalid streamed advance");
+  INSEM_REQUIRE(n_sources == 0 || amp_in, INSEM_CUDA_ERR_INVALID, "missing source amplitudes");
+  if (!initialized) initialize();
+  ensure_graph();
+  const int32_t todo = std::min<int32_t>(n, n_steps - step);
+  int32_t rows = 0;
+  CUDA_CHECK(cudaEventRecord(ev0, stream));
+  for (int32_t k = 0; k < todo; ++k) {
+    const int32_t s = step + 1 + k;
+    for (int q = 0; q < n_sources; ++q)
+      CUDA_CHECK(cudaMemcpyAsync(src_amp.get() + static_cast<std::size_t>(q) * n_amp + s,
+                                 amp_in + static_cast<std::size_t>(k) * n_sources + q, sizeof(float),
+                                 cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaGraphLaunch(graph_exec, stream));
+    if (s % record_every == 0 && rows_out && n_cols > 0) {
+      CUDA_CHECK(cudaMemcpyAsync(rows_out + static_cast<std::size_t>(rows) * n_cols,
+                                 trace_buf.get() + static_cast<std::size_t>(s / record_every) * n_cols,
+                                 n_cols * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      ++rows;
+    }
+  }
+  CUDA_CHECK(cudaEventRecord(ev1, stream));
+  CUDA_CHECK(cudaStreamSynchronize(stream));
+  step += todo;
+  float ms = 0.0f;
+  CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+  last_ms = ms;
+  *n_rows = rows;
 }
 
 int32_t Solver::n_samples() const { return initialized ? step / record_every + 1 : 0; }
@@ -750,6 +797,25 @@ int insem_cuda_solver_internal_forces(insem_cuda_solver* h, int32_t domain, cons
     CUDA_CHECK(cudaStreamSynchronize(s.stream));
     CUDA_CHECK(cudaMemcpy(f, df.get(), n * sizeof(float), cudaMemcpyDeviceToHost));
   });
+}
+
+int insem_cuda_solver_advance_streamed(insem_cuda_solver* h, int32_t n, const float* amp_in, double* rows_out,
+                                       int32_t* n_rows) {
+  return guarded([&] {
+    INSEM_REQUIRE(h, INSEM_CUDA_ERR_INVALID, "null handle");
+    h->s->advance_streamed(n, amp_in, rows_out, n_rows);
+  });
+}
+
+int32_t insem_cuda_solver_n_columns(const insem_cuda_solver* h) { return h ? h->s->n_columns() : -1; }
+
+int32_t insem_cuda_solver_kernels_per_step(insem_cuda_solver* h) {
+  if (!h) return -1;
+  const int rc = guarded([&] {
+    DeviceGuard dg(h->s->device);
+    h->s->ensure_graph();
+  });
+  return rc == INSEM_CUDA_OK ? h->s->kernels_per_step : -1;
 }
 
 int insem_cuda_stable_dt(const insem_cuda_problem* problem, int32_t device, double* stable_dt) {

@@ -48,6 +48,10 @@ class Solver {
 
   void set_state(int32_t medium, const double* u, const double* v);
   void advance(int32_t n);
+  void advance_streamed(int32_t n, const float* amp_in, double* rows_out, int32_t* n_rows);
+  void ensure_graph();
+  int32_t kernels_per_step = 0;
+  int32_t n_columns() const { return n_cols; }
   int32_t n_samples() const;
   int32_t n_energy() const;
   void copy_trace(int32_t t, double* out);

@@ -79,6 +79,24 @@ class Solver:
     def run(self) -> None:
         N.check(N.lib().insem_cuda_solver_run(self._h))
 
+    def advance_streamed(self, n_steps: int, amplitudes: np.ndarray, rows_out: np.ndarray) -> int:
+        """n steps with per-step source amplitudes in ([n][n_sources] float32, host) and
+        the recorded rows out ([>= n / record_every][n_columns] float64, host)."""
+        assert amplitudes.dtype == np.float32 and amplitudes.flags.c_contiguous
+        assert rows_out.dtype == np.float64 and rows_out.flags.c_contiguous
+        n = C.c_int32()
+        N.check(N.lib().insem_cuda_solver_advance_streamed(self._h, int(n_steps), amplitudes.ctypes.data_as(N.f32p),
+                                                           rows_out.ctypes.data_as(N.f64p), C.byref(n)))
+        return n.value
+
+    @property
+    def n_columns(self) -> int:
+        return int(N.lib().insem_cuda_solver_n_columns(self._h))
+
+    @property
+    def kernels_per_step(self) -> int:
+        return int(N.lib().insem_cuda_solver_kernels_per_step(self._h))
+
     # ------------------------------------------------------------- state
     def _domain(self, medium: str) -> int:
         di = self.problem.domain_index(medium)

@@ -273,6 +273,18 @@ int insem_cuda_solver_state(insem_cuda_solver* h, int32_t domain, double* u, dou
 double insem_cuda_solver_last_advance_ms(const insem_cuda_solver* h);
 /* Internal forces f = -K u of a domain for a host field (Solver::internal_forces). */
 int insem_cuda_solver_internal_forces(insem_cuda_solver* h, int32_t domain, const float* u, float* f);
+/* Streamed advance: n steps where every step first copies that step's source
+ * amplitudes amp_in[s * n_sources + k] (host, pinned for best speed) to the
+ * device and, on record steps, copies the recorded sample row back to
+ * rows_out[r * n_columns ...] (host); *n_rows receives the rows written.
+ * Amplitudes given here replace the ones computed from the source time
+ * functions for those steps.  One synchronisation at the end. */
+int insem_cuda_solver_advance_streamed(insem_cuda_solver* h, int32_t n, const float* amp_in, double* rows_out,
+                                       int32_t* n_rows);
+/* Columns of a recorded sample row (all traces side by side, in trace order). */
+int32_t insem_cuda_solver_n_columns(const insem_cuda_solver* h);
+/* Kernel launches of one captured step (the step graph's kernel nodes). */
+int32_t insem_cuda_solver_kernels_per_step(insem_cuda_solver* h);
 
 /* ------------------------------------------------------------ stable dt */
 /* Power iteration for lambda_max(M^-1 K) with the reference's seeds and

@@ -113,3 +113,26 @@ def test_stable_dt(pkg, case):
     prob = pkg.ProblemData.from_npz(z)
     dt = estimate_stable_dt(prob)
     assert abs(dt - prob.stable_dt) <= 1e-6 * prob.stable_dt, (dt, prob.stable_dt)
+
+
+@pytest.mark.parametrize("case", ["c1", "lay", "bh1"])
+def test_streamed_advance_matches_traces(pkg, case):
+    """Per-step amplitudes in / sample rows out give the same samples as the plain run."""
+    from insem_b200.stf import amplitudes
+
+    z = golden(case)
+    prob = pkg.ProblemData.from_npz(z)
+    with pkg.Solver(prob) as s:
+        s.advance(3)
+        n = prob.n_steps - 3
+        amp = np.ascontiguousarray(amplitudes(prob, 4, n))
+        rows = np.zeros((n // prob.record_every + 1, s.n_columns))
+        got = s.advance_streamed(n, amp, rows)
+        assert s.step == prob.n_steps
+        assert s.kernels_per_step > 5
+    cols = []
+    for name, q in prob.trace_list():
+        cols.append(z[f"run.trace.{name}.{q}"])
+    full = np.concatenate(cols, axis=1)
+    first = 3 // prob.record_every + 1
+    assert np.array_equal(rows[:got], full[first:first + got])
