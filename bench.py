@@ -200,11 +200,11 @@ def run_ours(args, world, rank, local, pg):
     total_steps = args.warmup + 2 * args.steps + 2
     model = K.config3(nx=args.nx, n_steps=total_steps)
     t0 = time.perf_counter()
-    prob = K.build(model, device=device)
+    prob = K.build(model, device=device, stable_dt=args.stable_dt)
     setup_s = time.perf_counter() - t0
-    solver = pkg.Solver(prob, device=device)
+    solver = pkg.Solver(prob, device=device, use_graphs=not args.no_graphs)
     solver.advance(args.warmup)
-    kps = solver.kernels_per_step
+    kps = solver.kernels_per_step if not args.no_graphs else None
 
     barrier(pg, device)
     with ClockSampler(device) as clocks:
@@ -216,6 +216,13 @@ def run_ours(args, world, rank, local, pg):
 
     # e2e: per-step amplitudes in from pinned memory, sample rows out, wall clock
     from insem_b200.stf import amplitudes
+
+    if args.no_e2e:
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": world * prob.n_global_total() * args.steps / (ms * 1e-3),
+                              "ms_per_step": ms / args.steps, "note": "profiling run (no e2e, no baseline)"}))
+        solver.close()
+        return
 
     s0 = solver.step
     amp = torch.empty((args.steps, len(prob.sources)), dtype=torch.float32).pin_memory()
@@ -244,7 +251,7 @@ def run_ours(args, world, rank, local, pg):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "traffic": None, "kernel": "whole step (all kernels of one step)",
                      "algorithmic_bytes_per_step": b_step, "peak_source": how},
-        "gpu_launches": kps * args.steps,
+        "gpu_launches": (kps or 0) * args.steps,
         "kernels_per_step": kps,
         "clocks": clocks.summary(),
     }
@@ -268,6 +275,10 @@ def main():
     ap.add_argument("--nx", type=int, default=1024)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the streamed end-to-end run")
+    ap.add_argument("--no-graphs", action="store_true", help="plain launches instead of the step graph")
+    ap.add_argument("--stable-dt", type=float, default=None,
+                    help="use this stable time step instead of the device power iteration (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup(args.gpus)
