@@ -49,7 +49,13 @@ const char* last_error();
                                 std::string(#expr) + ": " + cudaGetErrorString(err__)); \
   } while (0)
 
-#define CUDA_LAUNCH_CHECK() CUDA_CHECK(cudaGetLastError())
+#define CUDA_LAUNCH_CHECK()                                                     \
+  do {                                                                          \
+    cudaError_t err__ = cudaGetLastError();                                     \
+    if (err__ != cudaSuccess)                                                   \
+      throw ::insem_b200::Error(INSEM_CUDA_ERR_CUDA, std::string("kernel launch at ") + __FILE__ + ":" + \
+                                std::to_string(__LINE__) + ": " + cudaGetErrorString(err__)); \
+  } while (0)
 
 // Runs `fn` and converts exceptions to a status code (C-ABI wrapper).
 template <class Fn>

@@ -154,62 +154,56 @@ __device__ __forceinline__ void load_metric(const float* metric, int b, int k, f
   }
 }
 
-// ------------------------------------------------------------------ fluxes
-// Phase 1 of an element: from the staged field su[c][k], the fluxes
-// f1/f2[c][k] (to shared memory), the point's direct (hoop) terms and, for
-// axial elements, the axis terms at i == 0 (to gx/gy).  `bb` is the block
-// element index, `kpt` = j * NG + i.
+// ------------------------------------------------------------- point math
+// Fluxes of one element point from its reference derivatives u_xi / u_eta
+// (per component), the point's own field values upt (hoop terms), and the
+// block data: f_xi / f_eta per component, the direct (hoop) terms, and for
+// axis points of axial elements the axis terms g xi_r, g eta_r (stored at
+// row j of gx*/gy*).  The body of each reference kernel's first loop.
 template <int NG, int KIND, bool ELASTIC, int M>
-__device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int kpt, bool axial,
-                                               const float* Dx, const float* Dy, const float* w2,
-                                               const float (*su)[NG * NG], float (*f1)[NG * NG],
-                                               float (*f2)[NG * NG], float* gx0, float* gy0, float* gx1,
-                                               float* gy1, float* direct) {
+__device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt, int i, int j, bool axial,
+                                           const float* uxi, const float* ueta, const float* upt, float* fx,
+                                           float* fy, float* direct, float* gx0, float* gy0, float* gx1,
+                                           float* gy1, float w2k) {
   constexpr int NPE = NG * NG;
-  const int i = kpt % NG, j = kpt / NG;
   if constexpr (KIND != INSEM_AXISYM) {
     float xi_x, xi_z, eta_x, eta_z, jac;
     load_metric<KIND, NPE>(blk.metric, bb, kpt, xi_x, xi_z, eta_x, eta_z, jac);
     const size_t p = static_cast<size_t>(bb) * NPE + kpt;
     if constexpr (ELASTIC) {
       // elastic_kernel (kernels.cpp:64-120)
-      float ux_xi, ux_eta, uz_xi, uz_eta;
-      ref_derivs<NG>(Dx, Dy, su[0], i, j, ux_xi, ux_eta);
-      ref_derivs<NG>(Dx, Dy, su[1], i, j, uz_xi, uz_eta);
       float ux_x, ux_z, uz_x, uz_z;
       if constexpr (KIND == INSEM_RECT) {
-        ux_x = fmul(ux_xi, xi_x);
-        ux_z = fmul(ux_eta, eta_z);
-        uz_x = fmul(uz_xi, xi_x);
-        uz_z = fmul(uz_eta, eta_z);
+        ux_x = fmul(uxi[0], xi_x);
+        ux_z = fmul(ueta[0], eta_z);
+        uz_x = fmul(uxi[1], xi_x);
+        uz_z = fmul(ueta[1], eta_z);
       } else {
-        phys_grad(ux_xi, ux_eta, xi_x, xi_z, eta_x, eta_z, ux_x, ux_z);
-        phys_grad(uz_xi, uz_eta, xi_x, xi_z, eta_x, eta_z, uz_x, uz_z);
+        phys_grad(uxi[0], ueta[0], xi_x, xi_z, eta_x, eta_z, ux_x, ux_z);
+        phys_grad(uxi[1], ueta[1], xi_x, xi_z, eta_x, eta_z, uz_x, uz_z);
       }
       float sxx, szz, sxz;
       el_stress(blk.coef0[p], blk.coef1[p], ux_x, ux_z, uz_x, uz_z, sxx, szz, sxz);
-      const float wj = fmul(w2[kpt], jac);
+      const float wj = fmul(w2k, jac);
       if constexpr (KIND == INSEM_RECT) {
-        f1[0][kpt] = fmul(fmul(wj, sxx), xi_x);
-        f1[1][kpt] = fmul(fmul(wj, sxz), xi_x);
-        f2[0][kpt] = fmul(fmul(wj, sxz), eta_z);
-        f2[1][kpt] = fmul(fmul(wj, szz), eta_z);
+        fx[0] = fmul(fmul(wj, sxx), xi_x);
+        fx[1] = fmul(fmul(wj, sxz), xi_x);
+        fy[0] = fmul(fmul(wj, sxz), eta_z);
+        fy[1] = fmul(fmul(wj, szz), eta_z);
       } else {
-        ref_flux(wj, sxx, sxz, xi_x, xi_z, eta_x, eta_z, f1[0][kpt], f2[0][kpt]);
-        ref_flux(wj, sxz, szz, xi_x, xi_z, eta_x, eta_z, f1[1][kpt], f2[1][kpt]);
+        ref_flux(wj, sxx, sxz, xi_x, xi_z, eta_x, eta_z, fx[0], fy[0]);
+        ref_flux(wj, sxz, szz, xi_x, xi_z, eta_x, eta_z, fx[1], fy[1]);
       }
     } else {
       // acoustic_kernel (kernels.cpp:122-158)
-      float p_xi, p_eta;
-      ref_derivs<NG>(Dx, Dy, su[0], i, j, p_xi, p_eta);
-      const float c = fmul(fmul(w2[kpt], jac), blk.coef0[p]);
+      const float c = fmul(fmul(w2k, jac), blk.coef0[p]);
       if constexpr (KIND == INSEM_RECT) {
-        f1[0][kpt] = fmul(fmul(fmul(c, p_xi), xi_x), xi_x);
-        f2[0][kpt] = fmul(fmul(fmul(c, p_eta), eta_z), eta_z);
+        fx[0] = fmul(fmul(fmul(c, uxi[0]), xi_x), xi_x);
+        fy[0] = fmul(fmul(fmul(c, ueta[0]), eta_z), eta_z);
       } else {
         float p_x, p_z;
-        phys_grad(p_xi, p_eta, xi_x, xi_z, eta_x, eta_z, p_x, p_z);
-        ref_flux(c, p_x, p_z, xi_x, xi_z, eta_x, eta_z, f1[0][kpt], f2[0][kpt]);
+        phys_grad(uxi[0], ueta[0], xi_x, xi_z, eta_x, eta_z, p_x, p_z);
+        ref_flux(c, p_x, p_z, xi_x, xi_z, eta_x, eta_z, fx[0], fy[0]);
       }
     }
   } else {
@@ -217,18 +211,13 @@ __device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int 
     const float* mt = blk.metric + static_cast<size_t>(bb) * 5 * NPE + kpt;
     const float xi_r = mt[0], xi_z = mt[NPE], eta_r = mt[2 * NPE], eta_z = mt[3 * NPE];
     const bool axis_pt = axial && i == 0;
-    // xi_r / eta_r at the axis point (0, j) of this row, for the axis spread.
     if constexpr (ELASTIC && M == 0) {
       // elastic_axisym_kernel (kernels.cpp:206-263)
-      float ur_xi, ur_eta, uz_xi, uz_eta;
-      ref_derivs<NG>(Dx, Dy, su[0], i, j, ur_xi, ur_eta);
-      ref_derivs<NG>(Dx, Dy, su[1], i, j, uz_xi, uz_eta);
       float ur_r, ur_z, uz_r, uz_z;
-      phys_grad(ur_xi, ur_eta, xi_r, xi_z, eta_r, eta_z, ur_r, ur_z);
-      phys_grad(uz_xi, uz_eta, xi_r, xi_z, eta_r, eta_z, uz_r, uz_z);
+      phys_grad(uxi[0], ueta[0], xi_r, xi_z, eta_r, eta_z, ur_r, ur_z);
+      phys_grad(uxi[1], ueta[1], xi_r, xi_z, eta_r, eta_z, uz_r, uz_z);
       const float r = blk.r[p];
-      const bool on_axis = r == 0.0f;
-      const float e_tt = on_axis ? ur_r : __fdiv_rn(su[0][kpt], r);
+      const float e_tt = r == 0.0f ? ur_r : __fdiv_rn(upt[0], r);
       const float lambda = blk.coef0[p], mu = blk.coef1[p];
       const float tr = fadd(fadd(ur_r, uz_z), e_tt);
       const float two_mu = fmul(2.0f, mu);
@@ -238,8 +227,8 @@ __device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int 
       const float stt = fadd(ltr, fmul(two_mu, e_tt));
       const float srz = fmul(mu, fadd(ur_z, uz_r));
       const float w = blk.wr[p];
-      ref_flux(w, srr, srz, xi_r, xi_z, eta_r, eta_z, f1[0][kpt], f2[0][kpt]);
-      ref_flux(w, srz, szz, xi_r, xi_z, eta_r, eta_z, f1[1][kpt], f2[1][kpt]);
+      ref_flux(w, srr, srz, xi_r, xi_z, eta_r, eta_z, fx[0], fy[0]);
+      ref_flux(w, srz, szz, xi_r, xi_z, eta_r, eta_z, fx[1], fy[1]);
       if (axis_pt) {
         direct[0] = 0.0f;
         const float g = fmul(w, stt);
@@ -250,27 +239,21 @@ __device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int 
       }
     } else if constexpr (!ELASTIC && M == 0) {
       // acoustic_axisym_kernel (kernels.cpp:265-294)
-      float p_xi, p_eta;
-      ref_derivs<NG>(Dx, Dy, su[0], i, j, p_xi, p_eta);
       float p_r, p_z;
-      phys_grad(p_xi, p_eta, xi_r, xi_z, eta_r, eta_z, p_r, p_z);
-      ref_flux(fmul(blk.wr[p], blk.coef0[p]), p_r, p_z, xi_r, xi_z, eta_r, eta_z, f1[0][kpt], f2[0][kpt]);
+      phys_grad(uxi[0], ueta[0], xi_r, xi_z, eta_r, eta_z, p_r, p_z);
+      ref_flux(fmul(blk.wr[p], blk.coef0[p]), p_r, p_z, xi_r, xi_z, eta_r, eta_z, fx[0], fy[0]);
     } else if constexpr (ELASTIC && M == 1) {
       // elastic_axisym1_kernel (kernels.cpp:305-385)
       const float s2 = 1.41421356237309504880f;
       const float is2 = 0.70710678118654752440f;
-      float up_xi, up_eta, um_xi, um_eta, uz_xi, uz_eta;
-      ref_derivs<NG>(Dx, Dy, su[0], i, j, up_xi, up_eta);
-      ref_derivs<NG>(Dx, Dy, su[1], i, j, um_xi, um_eta);
-      ref_derivs<NG>(Dx, Dy, su[2], i, j, uz_xi, uz_eta);
       float up_r, up_z, um_r, um_z, uz_r, uz_z;
-      phys_grad(up_xi, up_eta, xi_r, xi_z, eta_r, eta_z, up_r, up_z);
-      phys_grad(um_xi, um_eta, xi_r, xi_z, eta_r, eta_z, um_r, um_z);
-      phys_grad(uz_xi, uz_eta, xi_r, xi_z, eta_r, eta_z, uz_r, uz_z);
+      phys_grad(uxi[0], ueta[0], xi_r, xi_z, eta_r, eta_z, up_r, up_z);
+      phys_grad(uxi[1], ueta[1], xi_r, xi_z, eta_r, eta_z, um_r, um_z);
+      phys_grad(uxi[2], ueta[2], xi_r, xi_z, eta_r, eta_z, uz_r, uz_z);
       const float r = blk.r[p];
       const bool on_axis = r == 0.0f;
-      const float up_over_r = on_axis ? up_r : __fdiv_rn(su[0][kpt], r);
-      const float uz_over_r = on_axis ? uz_r : __fdiv_rn(su[2][kpt], r);
+      const float up_over_r = on_axis ? up_r : __fdiv_rn(upt[0], r);
+      const float uz_over_r = on_axis ? uz_r : __fdiv_rn(upt[2], r);
       const float ur_r = fmul(fadd(up_r, um_r), is2), ur_z = fmul(fadd(up_z, um_z), is2);
       const float ut_r = fmul(fsub(up_r, um_r), is2), ut_z = fmul(fsub(up_z, um_z), is2);
       const float e_tt = fmul(s2, up_over_r);
@@ -285,11 +268,9 @@ __device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int 
       const float srt = fmul(mu, fsub(ut_r, fmul(s2, up_over_r)));
       const float stz = fmul(mu, fsub(ut_z, uz_over_r));
       const float w = blk.wr[p];
-      ref_flux(w, fmul(fadd(srr, srt), is2), fmul(fadd(srz, stz), is2), xi_r, xi_z, eta_r, eta_z, f1[0][kpt],
-               f2[0][kpt]);
-      ref_flux(w, fmul(fsub(srr, srt), is2), fmul(fsub(srz, stz), is2), xi_r, xi_z, eta_r, eta_z, f1[1][kpt],
-               f2[1][kpt]);
-      ref_flux(w, srz, szz, xi_r, xi_z, eta_r, eta_z, f1[2][kpt], f2[2][kpt]);
+      ref_flux(w, fmul(fadd(srr, srt), is2), fmul(fadd(srz, stz), is2), xi_r, xi_z, eta_r, eta_z, fx[0], fy[0]);
+      ref_flux(w, fmul(fsub(srr, srt), is2), fmul(fsub(srz, stz), is2), xi_r, xi_z, eta_r, eta_z, fx[1], fy[1]);
+      ref_flux(w, srz, szz, xi_r, xi_z, eta_r, eta_z, fx[2], fy[2]);
       const float cp = fmul(s2, fsub(stt, srt));
       const float cz = -stz;
       if (axis_pt) {
@@ -306,20 +287,18 @@ __device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int 
       }
     } else {
       // acoustic_axisym1_kernel (kernels.cpp:389-431)
-      float p_xi, p_eta;
-      ref_derivs<NG>(Dx, Dy, su[0], i, j, p_xi, p_eta);
       float p_r, p_z;
-      phys_grad(p_xi, p_eta, xi_r, xi_z, eta_r, eta_z, p_r, p_z);
+      phys_grad(uxi[0], ueta[0], xi_r, xi_z, eta_r, eta_z, p_r, p_z);
       const float inv_rho = blk.coef0[p];
       const float wri = fmul(blk.wr[p], inv_rho);
-      ref_flux(wri, p_r, p_z, xi_r, xi_z, eta_r, eta_z, f1[0][kpt], f2[0][kpt]);
+      ref_flux(wri, p_r, p_z, xi_r, xi_z, eta_r, eta_z, fx[0], fy[0]);
       if (axis_pt) {
         direct[0] = 0.0f;
         const float g = fmul(wri, p_r);
         gx0[j] = fmul(g, xi_r);
         gy0[j] = fmul(g, eta_r);
       } else {
-        direct[0] = __fdiv_rn(fmul(fmul(blk.hoop[p], inv_rho), su[0][kpt]), blk.r[p]);
+        direct[0] = __fdiv_rn(fmul(fmul(blk.hoop[p], inv_rho), upt[0]), blk.r[p]);
       }
     }
   }
@@ -328,20 +307,77 @@ __device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int 
 // spread_axis_term (kernels.cpp:195-204) as seen from point (ia, ja): the
 // row-jq update (f -= g_jq xi_r Dx[ia]) reaches the points of row ja; the
 // column update (f -= g_jq eta_r Dy[jq][ja]) reaches column 0 for every jq,
-// after that jq's row update.
-template <int NG>
-__device__ __forceinline__ float axis_spread(float f, int ia, int ja, const float* Dx, const float* Dy,
-                                             const float* gx, const float* gy) {
-  if (ia != 0) return fsub(f, fmul(gx[ja], Dx[ia]));
+// after that jq's row update.  dx_row0 = Dx[ia] (row 0 of Dx); dy(q) =
+// Dy[q] with q = jq * NG + ja.
+template <int NG, class DyFn>
+__device__ __forceinline__ float axis_spread(float f, int ia, int ja, float dx_row0, DyFn dy, const float* gx,
+                                             const float* gy) {
+  if (ia != 0) return fsub(f, fmul(gx[ja], dx_row0));
 #pragma unroll
   for (int jq = 0; jq < NG; ++jq) {
-    if (jq == ja) f = fsub(f, fmul(gx[jq], Dx[0]));
-    f = fsub(f, fmul(gy[jq], Dy[jq * NG + ja]));
+    if (jq == ja) f = fsub(f, fmul(gx[jq], dx_row0));
+    f = fsub(f, fmul(gy[jq], dy(jq * NG + ja)));
   }
   return f;
 }
 
-// Phase 2 of an element: f[c] at point kpt from the staged fluxes.
+// Force of one element point from its weak divergence sums s[c] (the second
+// loop of each reference kernel): negation, hoop term, axis spread.
+template <int NG, int KIND, bool ELASTIC, int M, class DyFn>
+__device__ __forceinline__ void point_divergence(int i, int j, bool axial, const float* s, const float* direct,
+                                                 float dx_row0, DyFn dy, const float* gx0, const float* gy0,
+                                                 const float* gx1, const float* gy1, float* out) {
+  using C = ElemCfg<NG, KIND, ELASTIC, M>;
+  if constexpr (KIND != INSEM_AXISYM) {
+#pragma unroll
+    for (int c = 0; c < C::NC; ++c) out[c] = -s[c];
+  } else if constexpr (ELASTIC && M == 0) {
+    out[0] = -fadd(s[0], direct[0]);
+    out[1] = -s[1];
+    if (axial) out[0] = axis_spread<NG>(out[0], i, j, dx_row0, dy, gx0, gy0);
+  } else if constexpr (!ELASTIC && M == 0) {
+    out[0] = -s[0];
+  } else if constexpr (ELASTIC && M == 1) {
+    out[0] = -fadd(s[0], direct[0]);
+    out[1] = -s[1];
+    out[2] = -fadd(s[2], direct[1]);
+    if (axial) {
+      out[0] = axis_spread<NG>(out[0], i, j, dx_row0, dy, gx0, gy0);
+      out[2] = axis_spread<NG>(out[2], i, j, dx_row0, dy, gx1, gy1);
+    }
+  } else {
+    out[0] = -fadd(s[0], direct[0]);
+    if (axial) out[0] = axis_spread<NG>(out[0], i, j, dx_row0, dy, gx0, gy0);
+  }
+}
+
+// ------------------------------------------- one-thread-per-point phases
+// Phase 1 of an element (point threads): derivatives from the staged field
+// su[c][k], then point_flux; fluxes to shared memory f1/f2[c][k].
+template <int NG, int KIND, bool ELASTIC, int M>
+__device__ __forceinline__ void element_fluxes(const BlockDev& blk, int bb, int kpt, bool axial,
+                                               const float* Dx, const float* Dy, const float* w2,
+                                               const float (*su)[NG * NG], float (*f1)[NG * NG],
+                                               float (*f2)[NG * NG], float* gx0, float* gy0, float* gx1,
+                                               float* gy1, float* direct) {
+  using C = ElemCfg<NG, KIND, ELASTIC, M>;
+  const int i = kpt % NG, j = kpt / NG;
+  float uxi[C::NC], ueta[C::NC], upt[C::NC], fx[C::NC], fy[C::NC];
+#pragma unroll
+  for (int c = 0; c < C::NC; ++c) {
+    ref_derivs<NG>(Dx, Dy, su[c], i, j, uxi[c], ueta[c]);
+    upt[c] = su[c][kpt];
+  }
+  point_flux<NG, KIND, ELASTIC, M>(blk, bb, kpt, i, j, axial, uxi, ueta, upt, fx, fy, direct, gx0, gy0, gx1, gy1,
+                                   w2[kpt]);
+#pragma unroll
+  for (int c = 0; c < C::NC; ++c) {
+    f1[c][kpt] = fx[c];
+    f2[c][kpt] = fy[c];
+  }
+}
+
+// Phase 2 of an element (point threads): f[c] at point kpt from the staged fluxes.
 template <int NG, int KIND, bool ELASTIC, int M>
 __device__ __forceinline__ void element_divergence(int kpt, bool axial, const float* Dx, const float* Dy,
                                                    const float (*f1)[NG * NG], const float (*f2)[NG * NG],
@@ -349,27 +385,11 @@ __device__ __forceinline__ void element_divergence(int kpt, bool axial, const fl
                                                    const float* gy1, const float* direct, float* out) {
   using C = ElemCfg<NG, KIND, ELASTIC, M>;
   const int i = kpt % NG, j = kpt / NG;
-  if constexpr (KIND != INSEM_AXISYM) {
+  float s[C::NC];
 #pragma unroll
-    for (int c = 0; c < C::NC; ++c) out[c] = -weak_div<NG>(Dx, Dy, f1[c], f2[c], i, j);
-  } else if constexpr (ELASTIC && M == 0) {
-    out[0] = -fadd(weak_div<NG>(Dx, Dy, f1[0], f2[0], i, j), direct[0]);
-    out[1] = -weak_div<NG>(Dx, Dy, f1[1], f2[1], i, j);
-    if (axial) out[0] = axis_spread<NG>(out[0], i, j, Dx, Dy, gx0, gy0);
-  } else if constexpr (!ELASTIC && M == 0) {
-    out[0] = -weak_div<NG>(Dx, Dy, f1[0], f2[0], i, j);
-  } else if constexpr (ELASTIC && M == 1) {
-    out[0] = -fadd(weak_div<NG>(Dx, Dy, f1[0], f2[0], i, j), direct[0]);
-    out[1] = -weak_div<NG>(Dx, Dy, f1[1], f2[1], i, j);
-    out[2] = -fadd(weak_div<NG>(Dx, Dy, f1[2], f2[2], i, j), direct[1]);
-    if (axial) {
-      out[0] = axis_spread<NG>(out[0], i, j, Dx, Dy, gx0, gy0);
-      out[2] = axis_spread<NG>(out[2], i, j, Dx, Dy, gx1, gy1);
-    }
-  } else {
-    out[0] = -fadd(weak_div<NG>(Dx, Dy, f1[0], f2[0], i, j), direct[0]);
-    if (axial) out[0] = axis_spread<NG>(out[0], i, j, Dx, Dy, gx0, gy0);
-  }
+  for (int c = 0; c < C::NC; ++c) s[c] = weak_div<NG>(Dx, Dy, f1[c], f2[c], i, j);
+  point_divergence<NG, KIND, ELASTIC, M>(i, j, axial, s, direct, Dx[i], [Dy](int q) { return Dy[q]; }, gx0, gy0, gx1,
+                                         gy1, out);
 }
 
 }  // namespace insem_b200

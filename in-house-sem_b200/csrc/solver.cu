@@ -133,6 +133,12 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
   const int32_t n_energy = energy_every > 0 ? n_steps / energy_every + 1 : 0;
   energy.resize(static_cast<std::size_t>(std::max(n_energy, 1)) * 3);
   energy.zero();
+  {
+    StepState hs{};
+    hs.kin_c = dt * dt / 8.0;
+    CUDA_CHECK(cudaMemcpy(st, &hs, sizeof(hs), cudaMemcpyHostToDevice));
+  }
+  if (!setup_only && opts.path != 1) build_tiled(p);
   CUDA_CHECK(cudaStreamSynchronize(nullptr));
   CUDA_CHECK(cudaDeviceSynchronize());
 }
@@ -140,6 +146,9 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
 Solver::~Solver() {
   DeviceGuard dg(device);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  for (auto& g : tgraph)
+    if (g) cudaGraphExecDestroy(g);
+  if (mode_host) cudaFreeHost(mode_host);
   if (st) cudaFree(st);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
@@ -191,6 +200,7 @@ void Solver::build_sources(const insem_cuda_problem& p) {
       amp[static_cast<std::size_t>(s) * n_amp + k] = static_cast<float>(stf_value(so.stf, k * dt));
   }
   src_amp.upload(amp);
+  src_per_point = per;
   src.resize(domains.size());
   for (std::size_t di = 0; di < domains.size(); ++di) {
     std::vector<int32_t> points, offsets{0}, which;
@@ -558,11 +568,27 @@ void Solver::set_state(int32_t medium, const double* u_in, const double* v_in) {
   for (int64_t z : d.host_zero) fu[z] = fv[z] = 0.0f;
   CUDA_CHECK(cudaMemcpy(d.u.get(), fu.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   CUDA_CHECK(cudaMemcpy(d.v.get(), fv.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  if (tiled) {
+    TiledDomain& t = tdom[di];
+    std::vector<float> pu(n), pv(n);
+    for (int c = 0; c < d.ncomp; ++c)
+      for (int32_t g = 0; g < d.ng; ++g) {
+        pu[static_cast<std::size_t>(c) * d.ng + t.perm[g]] = fu[static_cast<std::size_t>(c) * d.ng + g];
+        pv[static_cast<std::size_t>(c) * d.ng + t.perm[g]] = fv[static_cast<std::size_t>(c) * d.ng + g];
+      }
+    CUDA_CHECK(cudaMemcpy(t.u_cur(parity), pu.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpy(t.v.get(), pv.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  }
 }
 
 void Solver::advance(int32_t n) {
   DeviceGuard dg(device);
   INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
+  if (tiled) {
+    int32_t dummy = 0;
+    advance_tiled(n, nullptr, nullptr, &dummy);
+    return;
+  }
   CUDA_CHECK(cudaEventRecord(ev0, stream));
   if (!initialized) initialize();
   const int32_t todo = std::min<int32_t>(n, n_steps - step);
@@ -626,6 +652,10 @@ void Solver::advance_streamed(int32_t n, const float* amp_in, double* rows_out, 
   DeviceGuard dg(device);
   INSEM_REQUIRE(n >= 0 && n_rows, INSEM_CUDA_ERR_INVALID, "invalid streamed advance");
   INSEM_REQUIRE(n_sources == 0 || amp_in, INSEM_CUDA_ERR_INVALID, "missing source amplitudes");
+  if (tiled) {
+    advance_tiled(n, amp_in, rows_out, n_rows);
+    return;
+  }
   if (!initialized) initialize();
   ensure_graph();
   const int32_t todo = std::min<int32_t>(n, n_steps - step);
@@ -677,6 +707,21 @@ void Solver::copy_state(int32_t di, double* u_out, double* v_out, double* a_out)
   INSEM_REQUIRE(di >= 0 && di < static_cast<int32_t>(domains.size()), INSEM_CUDA_ERR_INVALID, "domain out of range");
   auto& d = domains[di];
   CUDA_CHECK(cudaStreamSynchronize(stream));
+  if (tiled && initialized) {
+    TiledDomain& t = tdom[di];
+    auto conv = [&](const float* dev, double* out) {
+      if (!out) return;
+      std::vector<float> h(static_cast<std::size_t>(d.ncomp) * d.ng);
+      CUDA_CHECK(cudaMemcpy(h.data(), dev, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
+      for (int c = 0; c < d.ncomp; ++c)
+        for (int32_t g = 0; g < d.ng; ++g)
+          out[static_cast<std::size_t>(c) * d.ng + g] = h[static_cast<std::size_t>(c) * d.ng + t.perm[g]];
+    };
+    conv(t.u_cur(parity), u_out);
+    conv(t.v.get(), v_out);
+    conv(t.a.get(), a_out);
+    return;
+  }
   auto conv = [&](DeviceBuffer<float>& b, double* out) {
     if (!out) return;
     const auto h = b.download();
@@ -685,6 +730,275 @@ void Solver::copy_state(int32_t di, double* u_out, double* v_out, double* a_out)
   conv(d.u, u_out);
   conv(d.v, v_out);
   conv(d.a, a_out);
+}
+
+// ------------------------------------------------------------ tiled path
+void Solver::build_tiled(const insem_cuda_problem& p) {
+  const std::size_t npe = static_cast<std::size_t>(ngll) * ngll;
+  set_constant_basis(ngll, host_vec(p.basis.D, npe), p.basis.Dj ? host_vec(p.basis.Dj, npe) : std::vector<float>{},
+                     host_vec(p.basis.w2, npe));
+  const int te = opts.tile_elements > 0 ? std::min(opts.tile_elements, tile_elements(ngll)) : tile_elements(ngll);
+  const auto fp = host_vec(p.coupling.fluid_points, n_cpl), sp = host_vec(p.coupling.solid_points, n_cpl);
+  tdom.resize(domains.size());
+  for (std::size_t di = 0; di < domains.size(); ++di) {
+    const insem_cuda_domain& d = p.domains[di];
+    SpecialTerms terms;
+    terms.sources = src_per_point[di];
+    for (int32_t i = 0; i < n_cpl; ++i) {
+      if (static_cast<int>(di) == fluid) terms.coupling[fp[i]].push_back(i);
+      if (static_cast<int>(di) == solid) terms.coupling[sp[i]].push_back(i);
+    }
+    const auto ap = host_vec(d.absorbing_points, d.n_absorbing);
+    for (int32_t i = 0; i < d.n_absorbing; ++i) terms.absorbing[ap[i]] = i;
+    const uint8_t all = static_cast<uint8_t>((1u << d.ncomp) - 1u);
+    for (int32_t g : host_vec(d.dirichlet_points, d.n_dirichlet)) terms.zero[g] |= all;
+    const auto axc = host_vec(d.axis_components, d.n_axis_components);
+    uint8_t axm = 0;
+    for (int32_t c : axc) axm |= static_cast<uint8_t>(1u << c);
+    if (axm)
+      for (int32_t g : host_vec(d.axis_points, d.n_axis)) terms.zero[g] |= axm;
+    for (int r = 0; r < p.n_receivers; ++r)
+      if (p.receivers[r].domain == static_cast<int>(di))
+        for (int32_t g : host_vec(p.receivers[r].points, p.receivers[r].n_points)) terms.receivers.push_back(g);
+    tdom[di].build(d, ngll, te, terms,
+                   host_vec(d.absorbing_coef, static_cast<std::size_t>(d.n_absorbing) * d.ncomp * d.ncomp));
+  }
+  if (n_cpl > 0) {
+    std::vector<int32_t> f(n_cpl), s(n_cpl);
+    for (int32_t i = 0; i < n_cpl; ++i) {
+      f[i] = tdom[fluid].perm[fp[i]];
+      s[i] = tdom[solid].perm[sp[i]];
+    }
+    tcpl_fluid.upload(f);
+    tcpl_solid.upload(s);
+  }
+  std::vector<int32_t> rp;
+  for (int r = 0; r < p.n_receivers; ++r)
+    for (int32_t g : host_vec(p.receivers[r].points, p.receivers[r].n_points))
+      rp.push_back(tdom[p.receivers[r].domain].perm[g]);
+  trec_points.upload(rp.empty() ? std::vector<int32_t>{0} : rp);
+  int base = 0;
+  for (std::size_t di = 0; di < tdom.size(); ++di) {
+    ep_tile[di] = base;
+    ep_ntile[di] = tdom[di].n_tiles;
+    base += tdom[di].n_tiles;
+    ep_halo[di] = base;
+    ep_nhalo[di] = ceil_div(std::max(tdom[di].n_halo, 1), 256);
+    base += ep_nhalo[di];
+  }
+  epart.resize(2 * static_cast<std::size_t>(std::max(base, 1)));
+  epart.zero();
+  CUDA_CHECK(cudaMallocHost(&mode_host, 4 * sizeof(int32_t)));
+  mode_host[0] = kModeNormal;
+  mode_host[1] = kModeFinal;
+  mode_host[2] = kModeInit;
+  tiled = true;
+}
+
+AllFields Solver::tiled_fields(int par) {
+  AllFields f{};
+  for (std::size_t i = 0; i < tdom.size() && i < 2; ++i)
+    f.d[i] = {tdom[i].u_cur(par), tdom[i].vn.get(), tdom[i].a.get(), tdom[i].ng};
+  return f;
+}
+
+void Solver::set_mode(int mode) {
+  if (mode == cur_mode) return;
+  CUDA_CHECK(cudaMemcpyAsync(&st->mode, mode_host + mode, sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+  cur_mode = mode;
+}
+
+// One step of the tiled path on the field buffers of `par` (init: step 0,
+// explicit damping, no step increment).
+void Solver::enqueue_tiled(int par, bool init) {
+  if (!init) {
+    advance_step_kernel<<<1, 1, 0, stream>>>(st);
+    CUDA_LAUNCH_CHECK();
+  }
+  StepScalars sc{static_cast<float>(dt), static_cast<float>(0.5 * dt), static_cast<float>(0.5 * dt * dt),
+                 energy_every};
+  for (std::size_t di = 0; di < tdom.size(); ++di) {
+    TiledDomain& t = tdom[di];
+    if (t.n_cslots > 0) {
+      constrained_gather_kernel<<<ceil_div(t.n_cslots, 128), 128, 0, stream>>>(
+          t.n_cslots, t.cs_row.get(), t.rows(), t.u_cur(par), t.ng, t.ncomp, t.cval.get());
+      CUDA_LAUNCH_CHECK();
+    }
+  }
+  for (int di : {solid, fluid}) {
+    if (di < 0) continue;
+    TiledDomain& t = tdom[di];
+    for (std::size_t b = 0; b < t.blocks.size(); ++b) {
+      TileLaunch a;
+      a.dom = &t;
+      a.block = static_cast<int>(b);
+      a.parity = par;
+      a.sc = sc;
+      a.st = st;
+      a.epartial = epart.get() + 2 * static_cast<std::size_t>(ep_tile[di]);
+      a.elastic = t.medium == INSEM_ELASTIC;
+      a.stream = stream;
+      launch_tiles(ngll, a);
+    }
+  }
+  const double h_damp = init ? 0.0 : 0.5 * dt;
+  CouplingDev cp{tcpl_fluid.get(), tcpl_solid.get(), cpl_cx.get(), cpl_cz.get()};
+  for (int di : {solid, fluid}) {
+    if (di < 0) continue;
+    TiledDomain& t = tdom[di];
+    if (t.n_halo == 0) continue;
+    const bool el = t.medium == INSEM_ELASTIC;
+    const float* other = nullptr;
+    int32_t other_ng = 0;
+    bool pm = false;
+    if (n_cpl > 0) {
+      if (el) {
+        other = tdom[fluid].u_cur(par);
+        other_ng = tdom[fluid].ng;
+        pm = t.m == 1;
+      } else {
+        other = tdom[solid].a.get();
+        other_ng = tdom[solid].ng;
+        pm = tdom[solid].m == 1;
+      }
+    }
+    const int grid = ceil_div(t.n_halo, 256);
+    double* ep = epart.get();
+    const int e0 = ep_halo[di];
+    const TiledDev tv = t.view(par);
+    const HaloDev hv = t.halo_view();
+    if (!el) {
+      halo_step_kernel<1, false><<<grid, 256, 0, stream>>>(tv, hv, cp, other, other_ng, pm, src_amp.get(), n_amp, sc,
+                                                           h_damp, st, ep, e0);
+    } else if (t.ncomp == 2) {
+      halo_step_kernel<2, true><<<grid, 256, 0, stream>>>(tv, hv, cp, other, other_ng, pm, src_amp.get(), n_amp, sc,
+                                                          h_damp, st, ep, e0);
+    } else {
+      halo_step_kernel<3, true><<<grid, 256, 0, stream>>>(tv, hv, cp, other, other_ng, pm, src_amp.get(), n_amp, sc,
+                                                          h_damp, st, ep, e0);
+    }
+    CUDA_LAUNCH_CHECK();
+  }
+  ReceiversDev rv = receivers_view();
+  rv.points = trec_points.get();
+  if (n_acoustic_rec > 0) {
+    particle_velocity_kernel<<<ceil_div(n_acoustic_rec, 64), 64, 0, stream>>>(rv, tiled_fields(par),
+                                                                              rec_acoustic.get(), n_acoustic_rec, dt,
+                                                                              init ? 1 : 0);
+    CUDA_LAUNCH_CHECK();
+  }
+  if (n_cols > 0) {
+    record_kernel<<<ceil_div(n_cols, 64), 64, 0, stream>>>(rv, tiled_fields(par), rec_cols.get(), n_cols, st,
+                                                            record_every, trace_buf.get(), max_samples);
+    CUDA_LAUNCH_CHECK();
+  }
+  if (energy_every > 0) {
+    // potential order: elastic first
+    const int d0 = solid >= 0 ? solid : fluid;
+    const int d1 = solid >= 0 ? fluid : -1;
+    const int n_dom = d1 >= 0 ? 2 : 1;
+    int4 s0{ep_tile[d0], ep_ntile[d0], ep_halo[d0], tdom[d0].n_halo > 0 ? ep_nhalo[d0] : 0};
+    int4 s1{0, 0, 0, 0};
+    if (d1 >= 0) s1 = int4{ep_tile[d1], ep_ntile[d1], ep_halo[d1], tdom[d1].n_halo > 0 ? ep_nhalo[d1] : 0};
+    tiled_energy_kernel<<<1, kReduceThreads, 0, stream>>>(epart.get(), n_dom, s0, s1, st, energy_every, dt,
+                                                          energy.get(), static_cast<int32_t>(energy.size() / 3));
+    CUDA_LAUNCH_CHECK();
+  }
+}
+
+void Solver::tiled_begin_steps() {
+  if (!complete) return;
+  for (auto& t : tdom) {
+    const int64_t n = static_cast<int64_t>(t.ncomp) * t.ng;
+    predictor_inplace_kernel<<<grid_for(n), 256, 0, stream>>>(t.u_cur(parity), t.v.get(), t.a.get(), n,
+                                                             static_cast<float>(dt), static_cast<float>(0.5 * dt),
+                                                             static_cast<float>(0.5 * dt * dt));
+    CUDA_LAUNCH_CHECK();
+  }
+  complete = false;
+}
+
+// advance(n) on the tiled path; with rows_out, the streamed variant (amplitudes
+// in, recorded rows out, per step).
+void Solver::advance_tiled(int32_t n, const float* amp_in, double* rows_out, int32_t* n_rows) {
+  const bool streamed = rows_out != nullptr || amp_in != nullptr;
+  CUDA_CHECK(cudaEventRecord(ev0, stream));
+  if (!initialized) {
+    set_mode(kModeInit);
+    enqueue_tiled(parity, true);
+    parity ^= 1;
+    complete = true;
+    initialized = true;
+  }
+  const int32_t todo = std::min<int32_t>(n, n_steps - step);
+  if (todo > 0 && opts.use_graphs && !tgraph[0]) {
+    for (int par = 0; par < 2; ++par) {
+      cudaGraph_t g = nullptr;
+      CUDA_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue_tiled(par, false);
+      } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      CUDA_CHECK(cudaStreamEndCapture(stream, &g));
+      if (par == 0) {
+        std::size_t nn = 0;
+        CUDA_CHECK(cudaGraphGetNodes(g, nullptr, &nn));
+        std::vector<cudaGraphNode_t> nodes(nn);
+        if (nn) CUDA_CHECK(cudaGraphGetNodes(g, nodes.data(), &nn));
+        kernels_per_step = 0;
+        for (auto nd : nodes) {
+          cudaGraphNodeType ty;
+          CUDA_CHECK(cudaGraphNodeGetType(nd, &ty));
+          if (ty == cudaGraphNodeTypeKernel) ++kernels_per_step;
+        }
+      }
+      CUDA_CHECK(cudaGraphInstantiate(&tgraph[par], g, 0));
+      CUDA_CHECK(cudaGraphDestroy(g));
+    }
+  }
+  int32_t rows = 0;
+  for (int32_t k = 0; k < todo; ++k) {
+    tiled_begin_steps();
+    set_mode(k == todo - 1 ? kModeFinal : kModeNormal);
+    const int32_t s = step + 1 + k;
+    if (amp_in)
+      for (int q = 0; q < n_sources; ++q)
+        CUDA_CHECK(cudaMemcpyAsync(src_amp.get() + static_cast<std::size_t>(q) * n_amp + s,
+                                   amp_in + static_cast<std::size_t>(k) * n_sources + q, sizeof(float),
+                                   cudaMemcpyHostToDevice, stream));
+    if (opts.use_graphs) CUDA_CHECK(cudaGraphLaunch(tgraph[parity], stream));
+    else enqueue_tiled(parity, false);
+    parity ^= 1;
+    if (rows_out && s % record_every == 0 && n_cols > 0) {
+      CUDA_CHECK(cudaMemcpyAsync(rows_out + static_cast<std::size_t>(rows) * n_cols,
+                                 trace_buf.get() + static_cast<std::size_t>(s / record_every) * n_cols,
+                                 n_cols * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      ++rows;
+    }
+  }
+  if (todo > 0) complete = true;
+  step += todo;
+  CUDA_CHECK(cudaEventRecord(ev1, stream));
+  if (opts.check_finite && !streamed) {
+    for (auto& t : tdom) {
+      const int64_t nn = static_cast<int64_t>(t.ncomp) * t.ng;
+      finite_check_kernel<<<grid_for(nn), 256, 0, stream>>>(t.u_cur(parity), nn, st);
+      CUDA_LAUNCH_CHECK();
+    }
+  }
+  CUDA_CHECK(cudaStreamSynchronize(stream));
+  float ms = 0.0f;
+  CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+  last_ms = ms;
+  *n_rows = rows;
+  if (opts.check_finite && !streamed) {
+    StepState hs;
+    CUDA_CHECK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
+    INSEM_REQUIRE(!hs.nonfinite, INSEM_CUDA_ERR_NONFINITE, "the solution contains NaN or Inf (unstable time step?)");
+  }
 }
 
 }  // namespace insem_b200
@@ -811,6 +1125,7 @@ int32_t insem_cuda_solver_n_columns(const insem_cuda_solver* h) { return h ? h->
 
 int32_t insem_cuda_solver_kernels_per_step(insem_cuda_solver* h) {
   if (!h) return -1;
+  if (h->s->tiled) return h->s->kernels_per_step;  // counted when the step graphs are captured
   const int rc = guarded([&] {
     DeviceGuard dg(h->s->device);
     h->s->ensure_graph();

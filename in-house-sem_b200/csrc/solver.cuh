@@ -6,6 +6,7 @@
 
 #include "device_data.cuh"
 #include "step_kernels.cuh"
+#include "tiled_path.cuh"
 
 namespace insem_b200 {
 
@@ -113,6 +114,27 @@ class Solver {
   StepState* st = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  // ------------------------------------------------------ tiled fused path
+ public:
+  bool tiled = false;  // the default path: tiles + halo kernel per step
+ private:
+  void build_tiled(const insem_cuda_problem& p);
+  void enqueue_tiled(int parity, bool init);
+  void tiled_begin_steps();      // predictor after a complete state
+  void set_mode(int mode);
+  void advance_tiled(int32_t n, const float* amp_in, double* rows_out, int32_t* n_rows);
+  AllFields tiled_fields(int parity);
+  std::vector<TiledDomain> tdom;
+  std::vector<std::map<int32_t, std::vector<std::pair<int32_t, std::vector<float>>>>> src_per_point;
+  DeviceBuffer<int32_t> tcpl_fluid, tcpl_solid, trec_points;
+  DeviceBuffer<double> epart;
+  int ep_tile[2] = {0, 0}, ep_halo[2] = {0, 0}, ep_ntile[2] = {0, 0}, ep_nhalo[2] = {0, 0};
+  cudaGraphExec_t tgraph[2] = {nullptr, nullptr};
+  int parity = 0;
+  bool complete = false;  // u, v, a hold step `step` (after an init or final step)
+  int cur_mode = -1;
+  int32_t* mode_host = nullptr;  // pinned {normal, final, init}
 };
 
 }  // namespace insem_b200

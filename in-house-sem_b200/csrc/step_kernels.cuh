@@ -18,10 +18,13 @@ constexpr int kReduceThreads = 256;
 struct StepState {
   int32_t step;           // current step index (after the predictor's increment)
   int32_t nonfinite;      // set when a NaN/Inf was found
+  int32_t mode;           // tiled path: 0 normal, 1 final (state complete), 2 initial
+  int32_t pad;
+  double kin_c;           // dt^2 / 8 of the kinetic energy (solver.cpp:903)
 };
 
 // u += dt v + dt^2/2 a; v += dt/2 a   (solver.cpp:929-933)
-__global__ void predictor_kernel(float* __restrict__ u, float* __restrict__ v, const float* __restrict__ a,
+static __global__ void predictor_kernel(float* __restrict__ u, float* __restrict__ v, const float* __restrict__ a,
                                  int64_t n, float rdt, float half_dt, float half_dt2) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
@@ -32,13 +35,13 @@ __global__ void predictor_kernel(float* __restrict__ u, float* __restrict__ v, c
 }
 
 // v += dt/2 a   (solver.cpp:942-943)
-__global__ void corrector_kernel(float* __restrict__ v, const float* __restrict__ a, int64_t n, float half_dt) {
+static __global__ void corrector_kernel(float* __restrict__ v, const float* __restrict__ a, int64_t n, float half_dt) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     v[i] = fadd(v[i], fmul(half_dt, a[i]));
 }
 
-__global__ void advance_step_kernel(StepState* st) { st->step += 1; }
+static __global__ void advance_step_kernel(StepState* st) { st->step += 1; }
 
 // Sources (solver.cpp:679-687), merged per global point: every point's
 // contributions are applied in source order, f += coef * amp.
@@ -52,7 +55,7 @@ struct SourcesDev {
   int32_t n_amp = 0;
 };
 
-__global__ void sources_kernel(SourcesDev s, const StepState* st, int step_override, float* __restrict__ f,
+static __global__ void sources_kernel(SourcesDev s, const StepState* st, int step_override, float* __restrict__ f,
                                int32_t n_global, int32_t ncomp) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= s.n_points) return;
@@ -68,7 +71,7 @@ __global__ void sources_kernel(SourcesDev s, const StepState* st, int step_overr
 }
 
 // add_coupling_forces, solid side (solver.cpp:700-715): traction p n_f.
-__global__ void coupling_solid_kernel(int32_t n, const int32_t* __restrict__ fluid_points,
+static __global__ void coupling_solid_kernel(int32_t n, const int32_t* __restrict__ fluid_points,
                                       const int32_t* __restrict__ solid_points, const float* __restrict__ cx,
                                       const float* __restrict__ cz, const float* __restrict__ p_fluid,
                                       float* __restrict__ f, int32_t ng, bool pm, bool serial) {
@@ -92,7 +95,7 @@ __global__ void coupling_solid_kernel(int32_t n, const int32_t* __restrict__ flu
 }
 
 // add_coupling_forces, fluid side (solver.cpp:716-726): -n_f . a_s.
-__global__ void coupling_fluid_kernel(int32_t n, const int32_t* __restrict__ fluid_points,
+static __global__ void coupling_fluid_kernel(int32_t n, const int32_t* __restrict__ fluid_points,
                                       const int32_t* __restrict__ solid_points, const float* __restrict__ cx,
                                       const float* __restrict__ cz, const float* __restrict__ a_solid,
                                       int32_t ngs, float* __restrict__ f, bool pm, bool serial) {
@@ -110,7 +113,7 @@ __global__ void coupling_fluid_kernel(int32_t n, const int32_t* __restrict__ flu
 }
 
 // a = f * inv_mass   (solver.cpp:735-738)
-__global__ void inv_mass_kernel(const float* __restrict__ f, const float* __restrict__ inv_mass,
+static __global__ void inv_mass_kernel(const float* __restrict__ f, const float* __restrict__ inv_mass,
                                 float* __restrict__ a, int32_t ng, int32_t ncomp) {
   const int64_t total = static_cast<int64_t>(ng) * ncomp;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
@@ -137,7 +140,7 @@ __device__ __forceinline__ void solve_spd_dev(int n, double* A, double* b) {
 }
 
 // Stacey points (solver.cpp:740-760): (M + h C) a = f - C v per point, in double.
-__global__ void stacey_kernel(int32_t n_abs, const int32_t* __restrict__ points, const float* __restrict__ coef,
+static __global__ void stacey_kernel(int32_t n_abs, const int32_t* __restrict__ points, const float* __restrict__ coef,
                               const float* __restrict__ mass, const float* __restrict__ f,
                               const float* __restrict__ v, float* __restrict__ a, int32_t ng, int32_t ncomp,
                               double h) {
@@ -160,7 +163,7 @@ __global__ void stacey_kernel(int32_t n_abs, const int32_t* __restrict__ points,
 }
 
 // apply_dirichlet (solver.hpp:57-65) on a flat list of component*n_global+point indices.
-__global__ void zero_kernel(int32_t n, const int64_t* __restrict__ idx, float* __restrict__ x) {
+static __global__ void zero_kernel(int32_t n, const int64_t* __restrict__ idx, float* __restrict__ x) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[idx[i]] = 0.0f;
 }
@@ -207,7 +210,7 @@ __device__ __forceinline__ double interp(const ReceiversDev& r, int32_t rec, con
 
 // Particle velocity of acoustic receivers: trapezoid of -grad(p)/rho.  With
 // init != 0 only prev_a is set (Solver::initialize, solver.cpp:883-893).
-__global__ void particle_velocity_kernel(ReceiversDev r, AllFields fl, const int32_t* __restrict__ acoustic_recv,
+static __global__ void particle_velocity_kernel(ReceiversDev r, AllFields fl, const int32_t* __restrict__ acoustic_recv,
                                          int32_t n_acoustic, double dt, int init) {
   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n_acoustic) return;
@@ -230,7 +233,7 @@ __global__ void particle_velocity_kernel(ReceiversDev r, AllFields fl, const int
   pv[1] = az;
 }
 
-__global__ void record_kernel(ReceiversDev r, AllFields fl, const RecordColumn* __restrict__ cols, int32_t n_cols,
+static __global__ void record_kernel(ReceiversDev r, AllFields fl, const RecordColumn* __restrict__ cols, int32_t n_cols,
                               const StepState* st, int32_t record_every, double* __restrict__ traces,
                               int32_t max_samples) {
   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -269,7 +272,7 @@ __device__ __forceinline__ double block_reduce(double v, double* sh) {
 }
 
 // partial[blockIdx] = sum_i (double)x[i] * (double)y[i], gated on energy steps.
-__global__ void dot_partial_kernel(const float* __restrict__ x, const float* __restrict__ y, int64_t n,
+static __global__ void dot_partial_kernel(const float* __restrict__ x, const float* __restrict__ y, int64_t n,
                                    const StepState* st, int32_t energy_every, int force, double* partial) {
   __shared__ double sh[kReduceThreads];
   if (!force && (energy_every <= 0 || st->step % energy_every != 0)) return;
@@ -282,7 +285,7 @@ __global__ void dot_partial_kernel(const float* __restrict__ x, const float* __r
 }
 
 // partial[blockIdx] = sum mass[g] (0.5 v v - c a a)   (kinetic_energy, solver.cpp:900-915)
-__global__ void kinetic_partial_kernel(const float* __restrict__ v, const float* __restrict__ a,
+static __global__ void kinetic_partial_kernel(const float* __restrict__ v, const float* __restrict__ a,
                                        const float* __restrict__ mass, int32_t ng, int32_t ncomp, double c,
                                        const StepState* st, int32_t energy_every, int force, double* partial) {
   __shared__ double sh[kReduceThreads];
@@ -301,7 +304,7 @@ __global__ void kinetic_partial_kernel(const float* __restrict__ v, const float*
 // energy[sample] = (time, kinetic, potential): kinetic = sum of the n_kin
 // partial sets 0..n_kin-1 (domain order), potential = -0.5 * each of the
 // n_pot dot sets stored from set 2 on (elastic first, solver.cpp:673-678).
-__global__ void energy_finalize_kernel(const double* partial, int n_kin, int n_pot, const StepState* st,
+static __global__ void energy_finalize_kernel(const double* partial, int n_kin, int n_pot, const StepState* st,
                                        int32_t energy_every, int force, double dt, double* energy,
                                        int32_t max_samples) {
   __shared__ double sh[kReduceThreads];
@@ -327,7 +330,7 @@ __global__ void energy_finalize_kernel(const double* partial, int n_kin, int n_p
 
 // ------------------------------------------------------- power iteration
 // partial[blockIdx] = sum mass[g] x x over [ncomp][ng]   (solver.cpp:597-601, 631-638)
-__global__ void mass_norm_partial_kernel(const float* __restrict__ x, const float* __restrict__ mass, int32_t ng,
+static __global__ void mass_norm_partial_kernel(const float* __restrict__ x, const float* __restrict__ mass, int32_t ng,
                                          int32_t ncomp, double* partial) {
   __shared__ double sh[kReduceThreads];
   const int64_t n = static_cast<int64_t>(ng) * ncomp;
@@ -342,7 +345,7 @@ __global__ void mass_norm_partial_kernel(const float* __restrict__ x, const floa
 }
 
 // x = (float)(-f * inv_mass); partial = sum y^2   (solver.cpp:603-609)
-__global__ void power_update_kernel(const float* __restrict__ f, const float* __restrict__ inv_mass,
+static __global__ void power_update_kernel(const float* __restrict__ f, const float* __restrict__ inv_mass,
                                     float* __restrict__ x, int32_t ng, int32_t ncomp, double* partial) {
   __shared__ double sh[kReduceThreads];
   const int64_t n = static_cast<int64_t>(ng) * ncomp;
@@ -358,14 +361,14 @@ __global__ void power_update_kernel(const float* __restrict__ f, const float* __
 }
 
 // x = (float)(src * scale)
-__global__ void scale_kernel(const float* __restrict__ src, float* __restrict__ x, int64_t n, double scale) {
+static __global__ void scale_kernel(const float* __restrict__ src, float* __restrict__ x, int64_t n, double scale) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     x[i] = static_cast<float>(dmul(static_cast<double>(src[i]), scale));
 }
 
 // Sets st->nonfinite if any entry of x is NaN or Inf.
-__global__ void finite_check_kernel(const float* __restrict__ x, int64_t n, StepState* st) {
+static __global__ void finite_check_kernel(const float* __restrict__ x, int64_t n, StepState* st) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     if (!isfinite(x[i])) {

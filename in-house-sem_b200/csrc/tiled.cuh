@@ -1,0 +1,580 @@
+// Tiled fused time step.
+//
+// Elements of each block are grouped into compact tiles (one CTA each).  A
+// tile kernel stages the field of the tile's points in shared memory,
+// computes every element's force vector, assembles the points whose
+// contributions all come from the tile ("complete" points) in shared memory,
+// and finishes them in the same pass: a = f / M, corrector, and the next
+// step's predictor, writing u^{n+1} to the other field buffer.  Contributions
+// to points shared with other tiles, constrained (hanging) slots and every
+// point carrying a boundary, coupling, source or receiver term go to a halo
+// buffer; a halo kernel finishes those points with the full reference logic.
+//
+// Bitwise parity with the reference: each point's contributions are summed
+// in ascending slot order (DofMap::assemble, dof_map.hpp:123-141).  Inside a
+// tile, slot s of point p carries its rank (position of s in p's ascending
+// slot list); ranks are accumulated phase by phase (rank 0 stores 0 + f,
+// rank r adds), so the sum is the reference's.  Halo points sum their halo
+// buffer entries in the reference's slot order from a CSR list.
+//
+// Element math: one thread per element column i (NG threads per element).
+// A column thread holds its column of the field, its f_eta column and the
+// xi-row / xi-column of the basis derivative matrix in registers; rows of the
+// field and of f_xi come from shared memory as broadcasts within an
+// element; D entries indexed by the unrolled loop counters come from the
+// constant bank.  Every sum keeps the reference's operand order.
+#pragma once
+
+#include "element_ops.cuh"
+#include "step_kernels.cuh"
+
+namespace insem_b200 {
+
+// GLL derivative matrix, GLJ derivative matrix and w_i w_j per ngll (2..9).
+static __constant__ float c_basis[8][3][81];
+
+enum StepMode : int32_t { kModeNormal = 0, kModeFinal = 1, kModeInit = 2 };
+
+// Slot descriptor bits.
+constexpr uint32_t kSlotPointMask = 0xffffu;      // tile point index
+constexpr int kSlotRankShift = 16;                // local assembly rank (0..254)
+constexpr uint32_t kSlotRankNone = 0xffu;          // not assembled in the tile
+constexpr uint32_t kSlotConstrained = 1u << 24;   // value from the constrained-slot list
+
+struct TileHdr {
+  int32_t be0;     // first element of the tile (block-local, tile order)
+  int32_t ne;      // elements
+  int32_t cbeg;    // first complete point (device numbering)
+  int32_t nc;      // complete points
+  int32_t ntp;     // tile points: nc complete + halo points the tile reads
+  int32_t hl_off;  // offset of the halo tile points in halo_tp
+  int32_t hb;      // first halo-buffer entry of the tile
+  int32_t nhs;     // halo slots (entries written to the halo buffer)
+  int32_t hs_off;  // offset into hs_slot
+  int32_t ncs;     // constrained slots of the tile
+  int32_t cs_off;  // offset into cs_slot / cs_idx
+  int32_t maxrank; // highest local rank
+};
+
+// One domain of the tiled path, in device numbering.
+struct TiledDev {
+  int32_t ng = 0;          // points
+  int32_t n_complete = 0;  // complete points are [0, n_complete)
+  int32_t n_hbuf = 0;      // halo buffer entries (per component)
+  int32_t n_cslots = 0;    // constrained slots of the domain
+  const float* inv_mass = nullptr;
+  const float* mass = nullptr;
+  const float* u_cur = nullptr;
+  float* u_nxt = nullptr;
+  float* v = nullptr;
+  float* a = nullptr;
+  float* vn = nullptr;     // v^n at halo points (receivers)
+  const uint32_t* sdesc = nullptr;  // [n_el_tiles * npe] slot descriptors, tile order
+  const TileHdr* tiles = nullptr;
+  const int32_t* halo_tp = nullptr; // device point of each halo tile point
+  const int32_t* hs_slot = nullptr; // tile-local slot (e * npe + k) of each halo entry
+  const int32_t* cs_slot = nullptr; // tile-local slot of each constrained slot
+  const int32_t* cs_idx = nullptr;  // its index into cval
+  const float* cval = nullptr;      // [ncomp][n_cslots] gathered constrained-slot values
+  float* hbuf = nullptr;            // [ncomp][n_hbuf]
+};
+
+struct StepScalars {
+  float rdt, half_dt, half_dt2;
+  int32_t energy_every;
+};
+
+template <int NG>
+struct TileCfg {
+  static constexpr int NPE = NG * NG;
+  static constexpr int TE = (256 / NG) > 64 ? 64 : (256 / NG);  // elements per tile (max)
+  static constexpr int THREADS = TE * NG;
+  static constexpr int ROW = (NG + 1) & ~1;                      // padded row stride (floats)
+};
+
+__device__ __forceinline__ float cbasis(int ng, int which, int idx) { return c_basis[ng - 2][which][idx]; }
+
+// Shared-memory layout of one tile CTA (dynamic; TP = tile point capacity).
+template <int NG, int NC>
+struct TileSmem {
+  using Cfg = TileCfg<NG>;
+  static constexpr int ROWS_PER_EL = NC * NG;                     // rows of one element
+  static constexpr int EL_FLOATS = ROWS_PER_EL * Cfg::ROW;
+  static size_t bytes(int tp) {
+    return sizeof(float) * (2 * static_cast<size_t>(NC) * tp + 2 * static_cast<size_t>(Cfg::TE) * EL_FLOATS +
+                            static_cast<size_t>(Cfg::TE) * 4 * 16);
+  }
+};
+
+// Mode-dependent completion of a point (solver.cpp:924-944 fused):
+//   normal: v = v_half + dt/2 a; u' = u + dt v + dt^2/2 a; v' = v + dt/2 a
+//   final:  v = v_half + dt/2 a; u' = u                      (state complete)
+//   init:   v unchanged;         u' = u                      (step 0)
+__device__ __forceinline__ void complete_point(int mode, const StepScalars& sc, float u, float vh, float a, float& u_out,
+                                               float& v_state, float& v_n) {
+  if (mode == kModeInit) {
+    v_n = vh;
+    v_state = vh;
+    u_out = u;
+    return;
+  }
+  const float vn = fadd(vh, fmul(sc.half_dt, a));
+  v_n = vn;
+  if (mode == kModeFinal) {
+    v_state = vn;
+    u_out = u;
+  } else {
+    u_out = fadd(u, fadd(fmul(sc.rdt, vn), fmul(sc.half_dt2, a)));
+    v_state = fadd(vn, fmul(sc.half_dt, a));
+  }
+}
+
+// Gathers the values of constrained slots (DofMap::gather rows, dof_map.hpp:110-115).
+static __global__ void constrained_gather_kernel(int32_t n, const int32_t* __restrict__ row_of, RowsDev rows,
+                                          const float* __restrict__ u, int32_t ng, int32_t ncomp, float* __restrict__ cval) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t r = row_of[i];
+  for (int c = 0; c < ncomp; ++c) {
+    float s = 0.0f;
+    for (int32_t q = rows.offsets[r]; q < rows.offsets[r + 1]; ++q)
+      s = fadd(s, fmul(rows.weights[q], u[static_cast<size_t>(c) * ng + rows.dofs[q]]));
+    cval[static_cast<size_t>(c) * n + i] = s;
+  }
+}
+
+// Predictor on the whole field, in place (start of an advance() after a final step).
+static __global__ void predictor_inplace_kernel(float* __restrict__ u, float* __restrict__ v, const float* __restrict__ a,
+                                         int64_t n, float rdt, float half_dt, float half_dt2) {
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const float vi = v[i], ai = a[i];
+    u[i] = fadd(u[i], fadd(fmul(rdt, vi), fmul(half_dt2, ai)));
+    v[i] = fadd(vi, fmul(half_dt, ai));
+  }
+}
+
+template <int NG, int KIND, bool EL, int M>
+static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
+    tile_step_kernel(BlockDev blk, TiledDev td, StepScalars sc, const StepState* __restrict__ st,
+                     double* __restrict__ epartial, int32_t tile0, int32_t tp_cap) {
+  using Cfg = TileCfg<NG>;
+  using CE = ElemCfg<NG, KIND, EL, M>;
+  constexpr int NC = CE::NC;
+  constexpr int NPE = NG * NG;
+  constexpr int ROW = Cfg::ROW;
+  constexpr bool AXI = KIND == INSEM_AXISYM;
+  extern __shared__ __align__(16) float smem[];
+  float* tu = smem;                                 // [NC][tp_cap]
+  float* tf = tu + NC * tp_cap;                     // [NC][tp_cap]
+  float* su = tf + NC * tp_cap;                     // [TE][NC][NG][ROW] field rows, later staging
+  float* sfx = su + Cfg::TE * NC * NG * ROW;        // [TE][NC][NG][ROW] f_xi rows
+  float* sax = sfx + Cfg::TE * NC * NG * ROW;       // [TE][4][16] axis terms (gx0, gy0, gx1, gy1)
+
+  const TileHdr th = td.tiles[tile0 + blockIdx.x];
+  const int tid = threadIdx.x;
+  const int mode = st->mode;
+  const int32_t step = st->step;
+  const bool energy = (mode == kModeInit) ? (sc.energy_every > 0) : (sc.energy_every > 0 && step % sc.energy_every == 0);
+
+  // 1. tile points: complete range, then halo points the tile reads
+  for (int t = tid; t < th.ntp; t += Cfg::THREADS) {
+    const int32_t g = t < th.nc ? th.cbeg + t : td.halo_tp[th.hl_off + t - th.nc];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) tu[c * tp_cap + t] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
+  }
+  __syncthreads();
+
+  const int el = tid / NG;
+  const int i = tid - el * NG;
+  const bool active = el < th.ne;
+  const int bb = th.be0 + el;                           // block-local element (tile order)
+  const uint32_t* desc = td.sdesc + static_cast<size_t>(bb) * NPE;
+  float* urow = su + el * (NC * NG * ROW);              // this element's rows
+  float* frow = sfx + el * (NC * NG * ROW);
+  float* ax = sax + el * 64;
+
+  // 2. element field rows (slots through their tile point or the constrained list)
+  uint32_t dsc[NG];
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+      dsc[j] = desc[j * NG + i];
+      if (!(dsc[j] & kSlotConstrained)) {
+        const int p = dsc[j] & kSlotPointMask;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) urow[(c * NG + j) * ROW + i] = tu[c * tp_cap + p];
+      }
+    }
+  }
+  for (int q = tid; q < th.ncs; q += Cfg::THREADS) {
+    const int32_t ls = td.cs_slot[th.cs_off + q];
+    const int32_t ci = td.cs_idx[th.cs_off + q];
+    const int e = ls / NPE, k = ls - e * NPE;
+    const int jj = k / NG, ii = k - jj * NG;
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      su[e * (NC * NG * ROW) + (c * NG + jj) * ROW + ii] = td.cval[static_cast<size_t>(c) * td.n_cslots + ci];
+  }
+  __syncthreads();
+
+  // 3. derivatives and fluxes, one column per thread
+  const bool axial = AXI && active && blk.axial[bb] != 0;
+  float dxr[NG], dxc[NG], w2c[NG];  // Dx row i, Dx column i, w_i w_j
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    dxr[l] = cbasis(NG, axial ? 1 : 0, i * NG + l);
+    dxc[l] = cbasis(NG, axial ? 1 : 0, l * NG + i);
+    w2c[l] = cbasis(NG, 2, l * NG + i);
+  }
+  float ucol[NC][NG], fe[NC][NG], dir[2][NG];
+  if (active) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+#pragma unroll
+      for (int j = 0; j < NG; ++j) ucol[c][j] = urow[(c * NG + j) * ROW + i];
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+      const int k = j * NG + i;
+      float uxi[NC], ueta[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float* row = urow + (c * NG + j) * ROW;
+        float a = 0.0f, b = 0.0f;
+#pragma unroll
+        for (int l = 0; l < NG; ++l) {
+          a = fadd(a, fmul(dxr[l], row[l]));
+          b = fadd(b, fmul(cbasis(NG, 0, j * NG + l), ucol[c][l]));
+        }
+        uxi[c] = a;
+        ueta[c] = b;
+      }
+      float fx[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
+      point_flux<NG, KIND, EL, M>(blk, bb, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
+                                  w2c[j]);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        frow[(c * NG + j) * ROW + i] = fx[c];
+        fe[c][j] = fy[c];
+      }
+      dir[0][j] = dr[0];
+      dir[1][j] = dr[1];
+    }
+  }
+  __syncthreads();
+
+  // 4. weak divergence (interleaved xi / eta terms), hoop and axis terms
+  float fo[NC][NG];
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+      float s[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float* row = frow + (c * NG + j) * ROW;
+        float acc = 0.0f;
+#pragma unroll
+        for (int l = 0; l < NG; ++l) {
+          acc = fadd(acc, fmul(dxc[l], row[l]));
+          acc = fadd(acc, fmul(cbasis(NG, 0, l * NG + j), fe[c][l]));
+        }
+        s[c] = acc;
+      }
+      const float drj[2] = {dir[0][j], dir[1][j]};
+      float out[NC];
+      point_divergence<NG, KIND, EL, M>(i, j, axial, s, drj, dxc[0], [](int q) { return cbasis(NG, 0, q); }, ax,
+                                        ax + 16, ax + 32, ax + 48, out);
+#pragma unroll
+      for (int c = 0; c < NC; ++c) fo[c][j] = out[c];
+    }
+  }
+  __syncthreads();  // su is reused below as halo staging
+
+  // 5. local assembly in the reference's slot order, halo staging
+  float* stage = su;
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+      const uint32_t rank = (dsc[j] >> kSlotRankShift) & 0xffu;
+      if (rank == kSlotRankNone || (dsc[j] & kSlotConstrained)) {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) stage[(el * NC + c) * NPE + j * NG + i] = fo[c][j];
+      }
+    }
+  }
+  for (int r = 0; r <= th.maxrank; ++r) {
+    if (active) {
+#pragma unroll
+      for (int j = 0; j < NG; ++j) {
+        const uint32_t rank = (dsc[j] >> kSlotRankShift) & 0xffu;
+        if (rank == static_cast<uint32_t>(r) && !(dsc[j] & kSlotConstrained)) {
+          const int p = dsc[j] & kSlotPointMask;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) {
+            float* t = tf + c * tp_cap + p;
+            *t = (r == 0) ? fadd(0.0f, fo[c][j]) : fadd(*t, fo[c][j]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+  // 6. halo contributions out (hbuf order = ascending slot order within the tile)
+  for (int q = tid; q < th.nhs; q += Cfg::THREADS) {
+    const int32_t ls = td.hs_slot[th.hs_off + q];
+    const int e = ls / NPE, k = ls - e * NPE;
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      td.hbuf[static_cast<size_t>(c) * td.n_hbuf + th.hb + q] = stage[(e * NC + c) * NPE + k];
+  }
+
+  // 7. complete points: a = f / M, corrector, predictor; energy partials
+  double kin = 0.0, pot = 0.0;
+  for (int t = tid; t < th.nc; t += Cfg::THREADS) {
+    const int32_t g = th.cbeg + t;
+    const float im = td.inv_mass[g];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const size_t gi = static_cast<size_t>(c) * td.ng + g;
+      const float f = tf[c * tp_cap + t];
+      const float a = fmul(f, im);
+      const float u = tu[c * tp_cap + t];
+      float u_out, v_state, v_n;
+      complete_point(mode, sc, u, td.v[gi], a, u_out, v_state, v_n);
+      td.u_nxt[gi] = u_out;
+      td.v[gi] = v_state;
+      if (mode != kModeNormal) td.a[gi] = a;
+      if (energy) {
+        pot = dadd(pot, dmul(static_cast<double>(u), static_cast<double>(f)));
+        const double vv = v_n, aa = a;
+        const double m = td.mass[g];
+        kin = dadd(kin, dmul(m, dsub(dmul(dmul(0.5, vv), vv), dmul(dmul(st->kin_c, aa), aa))));
+      }
+    }
+  }
+  if (energy) {
+    // deterministic CTA reduction: warp shuffles in a fixed tree, then warps in order
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      kin = dadd(kin, __shfl_down_sync(0xffffffffu, kin, off));
+      pot = dadd(pot, __shfl_down_sync(0xffffffffu, pot, off));
+    }
+    __shared__ double wk[16], wp[16];
+    const int w = tid >> 5;
+    if ((tid & 31) == 0) {
+      wk[w] = kin;
+      wp[w] = pot;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double k2 = 0.0, p2 = 0.0;
+      for (int q = 0; q < (Cfg::THREADS + 31) / 32; ++q) {
+        k2 = dadd(k2, wk[q]);
+        p2 = dadd(p2, wp[q]);
+      }
+      epartial[2 * (tile0 + blockIdx.x)] = k2;
+      epartial[2 * (tile0 + blockIdx.x) + 1] = p2;
+    }
+  }
+}
+
+
+// ------------------------------------------------------------ halo kernel
+// Special-point records of a domain's halo points.
+struct HaloDev {
+  int32_t n = 0;                     // halo points: device points [n_complete, n_complete + n)
+  const int32_t* off = nullptr;      // [n+1] halo-buffer contributions, ascending slot order
+  const int32_t* pos = nullptr;      // halo-buffer entry of each contribution
+  const float* w = nullptr;          // its weight (constrained maps), nullptr when all are 1
+  const int32_t* spec = nullptr;     // [n] special record or -1
+  const int32_t* src_off = nullptr;  // [n_spec+1] source contributions of each record
+  const int32_t* src_which = nullptr;// source index of each contribution (row of the amplitude table)
+  const float* src_coef = nullptr;   // [contributions][ncomp]
+  const int32_t* cpl_off = nullptr;  // [n_spec+1] coupling entries of each record
+  const int32_t* cpl_idx = nullptr;
+  const int32_t* abs_idx = nullptr;  // [n_spec] Stacey index or -1
+  const float* abs_coef = nullptr;   // [n_abs][ncomp*ncomp]
+  const uint8_t* zero = nullptr;     // [n_spec] components set to zero (Dirichlet, axis)
+};
+
+// Fluid-solid interface in device numbering of both domains.
+struct CouplingDev {
+  const int32_t* fluid = nullptr;
+  const int32_t* solid = nullptr;
+  const float* cx = nullptr;
+  const float* cz = nullptr;
+};
+
+// Finishes the halo points of one domain: the assembled force from the halo
+// buffer, then (solver.cpp:669-762) sources, coupling, a = f / M or the
+// implicit Stacey solve, Dirichlet / axis zeros, and the mode's update.
+// `other` is the fluid's current pressure (solid domain) or the solid's new
+// acceleration (fluid domain), in that domain's device numbering.
+template <int NC, bool ELASTIC>
+static __global__ void __launch_bounds__(256)
+    halo_step_kernel(TiledDev td, HaloDev hd, CouplingDev cp, const float* __restrict__ other, int32_t other_ng,
+                     bool pm, const float* __restrict__ amp, int32_t n_amp, StepScalars sc, double h_damp,
+                     const StepState* __restrict__ st, double* __restrict__ epartial, int32_t epart0) {
+  const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  const int mode = st->mode;
+  const int32_t step = st->step;
+  const bool energy = (mode == kModeInit) ? (sc.energy_every > 0) : (sc.energy_every > 0 && step % sc.energy_every == 0);
+  double kin = 0.0, pot = 0.0;
+  if (h < hd.n) {
+    const int32_t g = td.n_complete + h;
+    float f[NC], a[NC];
+    const int32_t b = hd.off[h], e = hd.off[h + 1];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      float s = 0.0f;
+      for (int32_t q = b; q < e; ++q) {
+        const float v = td.hbuf[static_cast<size_t>(c) * td.n_hbuf + hd.pos[q]];
+        s = fadd(s, hd.w ? fmul(hd.w[q], v) : v);
+      }
+      f[c] = s;
+      if (energy) pot = dadd(pot, dmul(static_cast<double>(td.u_cur[static_cast<size_t>(c) * td.ng + g]),
+                                       static_cast<double>(s)));
+    }
+    const int32_t sp = hd.spec[h];
+    int32_t ai = -1;
+    uint8_t zmask = 0;
+    if (sp >= 0) {
+      for (int32_t q = hd.src_off[sp]; q < hd.src_off[sp + 1]; ++q) {
+        const float am = amp[static_cast<size_t>(hd.src_which[q]) * n_amp + step];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) f[c] = fadd(f[c], fmul(hd.src_coef[static_cast<size_t>(q) * NC + c], am));
+      }
+      const float hs = static_cast<float>(kSqrtHalf);
+      for (int32_t q = hd.cpl_off[sp]; q < hd.cpl_off[sp + 1]; ++q) {
+        const int32_t ci = hd.cpl_idx[q];
+        if constexpr (ELASTIC) {
+          const float p = other[cp.fluid[ci]];
+          if (pm) {
+            const float t = fmul(fmul(hs, cp.cx[ci]), p);
+            f[0] = fadd(f[0], t);
+            f[1] = fadd(f[1], t);
+          } else {
+            f[0] = fadd(f[0], fmul(cp.cx[ci], p));
+          }
+          f[NC - 1] = fadd(f[NC - 1], fmul(cp.cz[ci], p));
+        } else {
+          const int32_t gs = cp.solid[ci];
+          const float ar = pm ? fmul(hs, fadd(other[gs], other[static_cast<size_t>(other_ng) + gs])) : other[gs];
+          const float az = other[static_cast<size_t>(pm ? 2 : 1) * other_ng + gs];
+          f[0] = fsub(f[0], fadd(fmul(cp.cx[ci], ar), fmul(cp.cz[ci], az)));
+        }
+      }
+      ai = hd.abs_idx[sp];
+      zmask = hd.zero[sp];
+    }
+    const float im = td.inv_mass[g];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) a[c] = fmul(f[c], im);
+    if (ai >= 0) {
+      const float* cc = hd.abs_coef + static_cast<size_t>(ai) * NC * NC;
+      double A[NC * NC], rhs[NC];
+      const double mass = td.mass[g];
+#pragma unroll
+      for (int r = 0; r < NC; ++r) {
+        rhs[r] = static_cast<double>(f[r]);
+#pragma unroll
+        for (int s2 = 0; s2 < NC; ++s2) {
+          rhs[r] = dsub(rhs[r], dmul(static_cast<double>(cc[r * NC + s2]),
+                                     static_cast<double>(td.v[static_cast<size_t>(s2) * td.ng + g])));
+          A[r * NC + s2] = dadd(dmul(h_damp, static_cast<double>(cc[r * NC + s2])), r == s2 ? mass : 0.0);
+        }
+      }
+      solve_spd_dev(NC, A, rhs);
+#pragma unroll
+      for (int r = 0; r < NC; ++r) a[r] = static_cast<float>(rhs[r]);
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      if (zmask & (1u << c)) a[c] = 0.0f;
+      const size_t gi = static_cast<size_t>(c) * td.ng + g;
+      float u_out, v_state, v_n;
+      const float u = td.u_cur[gi];
+      complete_point(mode, sc, u, td.v[gi], a[c], u_out, v_state, v_n);
+      td.u_nxt[gi] = u_out;
+      td.v[gi] = v_state;
+      td.a[gi] = a[c];
+      td.vn[gi] = v_n;
+      if (energy) {
+        const double vv = v_n, aa = a[c];
+        kin = dadd(kin, dmul(static_cast<double>(td.mass[g]), dsub(dmul(dmul(0.5, vv), vv), dmul(dmul(st->kin_c, aa), aa))));
+      }
+    }
+  }
+  if (energy) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      kin = dadd(kin, __shfl_down_sync(0xffffffffu, kin, off));
+      pot = dadd(pot, __shfl_down_sync(0xffffffffu, pot, off));
+    }
+    __shared__ double wk[8], wp[8];
+    if ((threadIdx.x & 31) == 0) {
+      wk[threadIdx.x >> 5] = kin;
+      wp[threadIdx.x >> 5] = pot;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double k2 = 0.0, p2 = 0.0;
+      for (int q = 0; q < 8; ++q) {
+        k2 = dadd(k2, wk[q]);
+        p2 = dadd(p2, wp[q]);
+      }
+      epartial[2 * (epart0 + blockIdx.x)] = k2;
+      epartial[2 * (epart0 + blockIdx.x) + 1] = p2;
+    }
+  }
+}
+
+// energy[sample] = (time, kinetic, potential) from the per-CTA partials of
+// the tiled step: kinetic sums all sets, potential = -0.5 x each domain's
+// u . f_int, elastic first (solver.cpp:673-678).  Partials of set d are
+// [start_d, start_d + count_d).
+static __global__ void tiled_energy_kernel(const double* __restrict__ epartial, int n_dom, int4 sets0, int4 sets1,
+                                    const StepState* __restrict__ st, int32_t energy_every, double dt,
+                                    double* __restrict__ energy, int32_t max_samples) {
+  __shared__ double sh[kReduceThreads];
+  const int mode = st->mode;
+  const int32_t step = st->step;
+  const bool on = (mode == kModeInit) ? (energy_every > 0) : (energy_every > 0 && step % energy_every == 0);
+  if (!on) return;
+  const int starts[4] = {sets0.x, sets0.z, sets1.x, sets1.z};
+  const int counts[4] = {sets0.y, sets0.w, sets1.y, sets1.w};
+  double kin = 0.0, pot = 0.0;
+  for (int d = 0; d < n_dom; ++d) {
+    double pk = 0.0, pp = 0.0;
+    // two partial sets per domain: tiles (set 2d) and halo (set 2d + 1)
+    for (int part = 0; part < 2; ++part) {
+      const int q = 2 * d + part;
+      double sk = 0.0, spp = 0.0;
+      for (int i = threadIdx.x; i < counts[q]; i += blockDim.x) {
+        sk = dadd(sk, epartial[2 * (starts[q] + i)]);
+        spp = dadd(spp, epartial[2 * (starts[q] + i) + 1]);
+      }
+      const double bk = block_reduce(sk, sh);
+      __syncthreads();
+      const double bp = block_reduce(spp, sh);
+      __syncthreads();
+      pk = dadd(pk, bk);
+      pp = dadd(pp, bp);
+    }
+    kin = dadd(kin, pk);
+    pot = dsub(pot, dmul(0.5, pp));
+  }
+  if (threadIdx.x == 0) {
+    const int32_t sample = energy_every > 0 ? step / energy_every : 0;
+    if (sample < max_samples) {
+      energy[sample * 3 + 0] = dmul(static_cast<double>(step), dt);
+      energy[sample * 3 + 1] = kin;
+      energy[sample * 3 + 2] = pot;
+    }
+  }
+}
+
+}  // namespace insem_b200

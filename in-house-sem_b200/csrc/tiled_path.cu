@@ -1,0 +1,473 @@
+// Tiling and device numbering of the tiled fused step (host side).
+//
+// Per domain:
+//   1. elements of each block are grown into compact tiles of <= TE elements
+//      (breadth-first over elements that share a global point);
+//   2. a point is "complete" when every contribution to it is an
+//      unconstrained slot of one tile and it carries no boundary, coupling,
+//      source, receiver, Dirichlet or axis term; all other points are halo
+//      points;
+//   3. device numbering: complete points tile by tile, then halo points
+//      (both in ascending reference order inside their group);
+//   4. slot descriptors give each slot its tile point and, for complete
+//      points, its rank in the point's ascending slot list (the order of
+//      DofMap::assemble, dof_map.hpp:123-141);
+//   5. halo slots write to a halo buffer whose entries each halo point sums
+//      through a CSR in ascending slot order (weights of constrained maps kept).
+#include <algorithm>
+#include <numeric>
+
+#include "tiled_path.cuh"
+
+namespace insem_b200 {
+
+void set_constant_basis_ng2(const float*, const float*, const float*);
+void set_constant_basis_ng3(const float*, const float*, const float*);
+void set_constant_basis_ng4(const float*, const float*, const float*);
+void set_constant_basis_ng5(const float*, const float*, const float*);
+void set_constant_basis_ng6(const float*, const float*, const float*);
+void set_constant_basis_ng7(const float*, const float*, const float*);
+void set_constant_basis_ng8(const float*, const float*, const float*);
+void set_constant_basis_ng9(const float*, const float*, const float*);
+int tile_elements_ng2();
+int tile_elements_ng3();
+int tile_elements_ng4();
+int tile_elements_ng5();
+int tile_elements_ng6();
+int tile_elements_ng7();
+int tile_elements_ng8();
+int tile_elements_ng9();
+
+void set_constant_basis(int ngll, const std::vector<float>& D, const std::vector<float>& Dj,
+                        const std::vector<float>& w2) {
+  const float* dj = Dj.empty() ? nullptr : Dj.data();
+  switch (ngll) {
+    case 2: set_constant_basis_ng2(D.data(), dj, w2.data()); break;
+    case 3: set_constant_basis_ng3(D.data(), dj, w2.data()); break;
+    case 4: set_constant_basis_ng4(D.data(), dj, w2.data()); break;
+    case 5: set_constant_basis_ng5(D.data(), dj, w2.data()); break;
+    case 6: set_constant_basis_ng6(D.data(), dj, w2.data()); break;
+    case 7: set_constant_basis_ng7(D.data(), dj, w2.data()); break;
+    case 8: set_constant_basis_ng8(D.data(), dj, w2.data()); break;
+    case 9: set_constant_basis_ng9(D.data(), dj, w2.data()); break;
+    default: check_ngll(ngll);
+  }
+}
+
+int tile_elements(int ngll) {
+  switch (ngll) {
+    case 2: return tile_elements_ng2();
+    case 3: return tile_elements_ng3();
+    case 4: return tile_elements_ng4();
+    case 5: return tile_elements_ng5();
+    case 6: return tile_elements_ng6();
+    case 7: return tile_elements_ng7();
+    case 8: return tile_elements_ng8();
+    case 9: return tile_elements_ng9();
+    default: check_ngll(ngll);
+  }
+  return 0;
+}
+
+void launch_tiles(int ngll, const TileLaunch& a) {
+  switch (ngll) {
+    case 2: launch_tiles_ng2(a); break;
+    case 3: launch_tiles_ng3(a); break;
+    case 4: launch_tiles_ng4(a); break;
+    case 5: launch_tiles_ng5(a); break;
+    case 6: launch_tiles_ng6(a); break;
+    case 7: launch_tiles_ng7(a); break;
+    case 8: launch_tiles_ng8(a); break;
+    case 9: launch_tiles_ng9(a); break;
+    default: check_ngll(ngll);
+  }
+}
+
+BlockDev TiledDomain::BlockTiles::view() const {
+  BlockDev v;
+  v.kind = kind;
+  v.m = m;
+  v.n = n;
+  v.metric = metric.get();
+  v.coef0 = coef0.get();
+  v.coef1 = coef1.get();
+  v.wr = wr.get();
+  v.hoop = hoop.get();
+  v.r = r.get();
+  v.axial = axial.get();
+  return v;
+}
+
+TiledDev TiledDomain::view(int parity) const {
+  TiledDev t;
+  t.ng = ng;
+  t.n_complete = n_complete;
+  t.n_hbuf = n_hbuf;
+  t.n_cslots = n_cslots;
+  t.inv_mass = inv_mass.get();
+  t.mass = mass.get();
+  t.u_cur = parity ? u1.get() : u0.get();
+  t.u_nxt = const_cast<float*>(parity ? u0.get() : u1.get());
+  t.v = const_cast<float*>(v.get());
+  t.a = const_cast<float*>(a.get());
+  t.vn = const_cast<float*>(vn.get());
+  t.sdesc = sdesc.get();
+  t.tiles = tiles.get();
+  t.halo_tp = halo_tp.get();
+  t.hs_slot = hs_slot.get();
+  t.cs_slot = cs_slot.get();
+  t.cs_idx = cs_idx.get();
+  t.cval = cval.get();
+  t.hbuf = const_cast<float*>(hbuf.get());
+  return t;
+}
+
+HaloDev TiledDomain::halo_view() const {
+  HaloDev h;
+  h.n = n_halo;
+  h.off = h_off.get();
+  h.pos = h_pos.get();
+  h.w = weighted ? h_w.get() : nullptr;
+  h.spec = h_spec.get();
+  h.src_off = src_off.get();
+  h.src_which = src_which.get();
+  h.src_coef = src_coef.get();
+  h.cpl_off = cpl_off.get();
+  h.cpl_idx = cpl_idx.get();
+  h.abs_idx = abs_idx.get();
+  h.abs_coef = abs_coef_d.get();
+  h.zero = zero.get();
+  return h;
+}
+
+void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const SpecialTerms& sp,
+                        const std::vector<float>& abs_coef_host) {
+  medium = d.medium;
+  ncomp = d.ncomp;
+  m = d.azimuthal_order;
+  ng = d.dofs.n_global;
+  npe = ngll * ngll;
+  n_elements = d.dofs.n_elements;
+  const std::size_t n_slots = static_cast<std::size_t>(n_elements) * npe;
+  const auto l2g = host_vec(d.dofs.l2g, n_slots);
+  const auto t_off = host_vec(d.dofs.t_offsets, static_cast<std::size_t>(ng) + 1);
+  const auto t_slots = host_vec(d.dofs.t_slots, static_cast<std::size_t>(t_off.back()));
+  weighted = d.dofs.n_rows > 0 && d.dofs.t_weights != nullptr;
+  const auto t_w = weighted ? host_vec(d.dofs.t_weights, static_cast<std::size_t>(t_off.back())) : std::vector<double>{};
+
+  // special points
+  std::vector<char> special(ng, 0);
+  for (const auto& kv : sp.sources) special[kv.first] = 1;
+  for (const auto& kv : sp.coupling) special[kv.first] = 1;
+  for (const auto& kv : sp.absorbing) special[kv.first] = 1;
+  for (const auto& kv : sp.zero) special[kv.first] = 1;
+  for (int32_t g : sp.receivers) special[g] = 1;
+
+  // 1. tiles per block
+  std::vector<int32_t> eblock(n_elements, -1), epos(n_elements, -1);
+  for (int b = 0; b < d.n_blocks; ++b)
+    for (int q = 0; q < d.blocks[b].n_elements; ++q) {
+      const int32_t e = d.blocks[b].elements[q];
+      INSEM_REQUIRE(e >= 0 && e < n_elements && eblock[e] < 0, INSEM_CUDA_ERR_INVALID, "block elements overlap");
+      eblock[e] = b;
+      epos[e] = q;
+    }
+  std::vector<int32_t> tile_of(n_elements, -1), stamp(n_elements, -1);
+  std::vector<std::vector<int32_t>> tile_elems;
+  std::vector<int32_t> tile_block;
+  blocks.clear();
+  blocks.resize(d.n_blocks);
+  std::vector<int32_t> queue;
+  for (int b = 0; b < d.n_blocks; ++b) {
+    blocks[b].kind = d.blocks[b].kind;
+    blocks[b].m = d.blocks[b].azimuthal_order;
+    blocks[b].n = d.blocks[b].n_elements;
+    blocks[b].tile0 = static_cast<int>(tile_elems.size());
+    for (int q = 0; q < d.blocks[b].n_elements; ++q) {
+      const int32_t seed = d.blocks[b].elements[q];
+      if (tile_of[seed] >= 0) continue;
+      const int32_t t = static_cast<int32_t>(tile_elems.size());
+      tile_elems.emplace_back();
+      tile_block.push_back(b);
+      auto& te_list = tile_elems.back();
+      queue.clear();
+      queue.push_back(seed);
+      stamp[seed] = t;
+      std::size_t head = 0;
+      while (head < queue.size() && static_cast<int>(te_list.size()) < te) {
+        const int32_t e = queue[head++];
+        tile_of[e] = t;
+        te_list.push_back(e);
+        for (int k = 0; k < npe; ++k) {
+          const int32_t g = l2g[static_cast<std::size_t>(e) * npe + k];
+          if (g < 0) continue;
+          for (int32_t s = t_off[g]; s < t_off[g + 1]; ++s) {
+            const int32_t e2 = t_slots[s] / npe;
+            if (eblock[e2] == b && tile_of[e2] < 0 && stamp[e2] != t) {
+              stamp[e2] = t;
+              queue.push_back(e2);
+            }
+          }
+        }
+      }
+      std::sort(te_list.begin(), te_list.end());
+    }
+    blocks[b].ntiles = static_cast<int>(tile_elems.size()) - blocks[b].tile0;
+  }
+  n_tiles = static_cast<int>(tile_elems.size());
+
+  // 2. point classification
+  std::vector<int32_t> owner(ng, -1);
+  for (int32_t g = 0; g < ng; ++g) {
+    if (special[g]) continue;
+    int32_t t = -2;
+    bool ok = true;
+    for (int32_t s = t_off[g]; s < t_off[g + 1] && ok; ++s) {
+      const int32_t slot = t_slots[s];
+      if (l2g[slot] != g) ok = false;
+      const int32_t tt = tile_of[slot / npe];
+      if (t == -2) t = tt;
+      else if (tt != t) ok = false;
+    }
+    if (ok && t >= 0) owner[g] = t;
+  }
+  // 3. device numbering
+  std::vector<int32_t> count(n_tiles + 1, 0);
+  for (int32_t g = 0; g < ng; ++g)
+    if (owner[g] >= 0) ++count[owner[g] + 1];
+  std::vector<int32_t> cbeg(n_tiles + 1, 0);
+  for (int t = 0; t < n_tiles; ++t) cbeg[t + 1] = cbeg[t] + count[t + 1];
+  n_complete = cbeg[n_tiles];
+  perm.assign(ng, -1);
+  {
+    std::vector<int32_t> fill(cbeg.begin(), cbeg.end() - 1);
+    int32_t h = n_complete;
+    for (int32_t g = 0; g < ng; ++g) perm[g] = owner[g] >= 0 ? fill[owner[g]]++ : h++;
+  }
+  n_halo = ng - n_complete;
+
+  // 4. ranks of complete points' slots
+  std::vector<uint8_t> rank_of(n_slots, 0xff);
+  for (int32_t g = 0; g < ng; ++g) {
+    if (owner[g] < 0) continue;
+    const int32_t nsl = t_off[g + 1] - t_off[g];
+    INSEM_REQUIRE(nsl < 255, INSEM_CUDA_ERR_UNSUPPORTED, "too many contributions to one point");
+    for (int32_t s = t_off[g]; s < t_off[g + 1]; ++s) rank_of[t_slots[s]] = static_cast<uint8_t>(s - t_off[g]);
+  }
+
+  // 5. per tile: tile points, descriptors, halo and constrained slots
+  std::vector<TileHdr> hdr(n_tiles);
+  std::vector<uint32_t> desc(n_slots);
+  std::vector<int32_t> htp, hslot, cslot, cidx, crow;
+  std::vector<int32_t> hpos_of_slot(n_slots, -1);
+  std::vector<int32_t> tpi(ng, -1), tpi_stamp(ng, -1);
+  std::vector<int32_t> block_elem_count(d.n_blocks, 0);
+  for (int b = 0; b < d.n_blocks; ++b) blocks[b].e_off = 0;
+  int32_t e_running = 0, hb = 0;
+  for (int b = 0; b < d.n_blocks; ++b) {
+    blocks[b].e_off = e_running;
+    int32_t be = 0;
+    for (int t = blocks[b].tile0; t < blocks[b].tile0 + blocks[b].ntiles; ++t) {
+      TileHdr& th = hdr[t];
+      th.be0 = be;
+      th.ne = static_cast<int32_t>(tile_elems[t].size());
+      th.cbeg = cbeg[t];
+      th.nc = cbeg[t + 1] - cbeg[t];
+      th.hl_off = static_cast<int32_t>(htp.size());
+      th.hs_off = static_cast<int32_t>(hslot.size());
+      th.cs_off = static_cast<int32_t>(cslot.size());
+      th.hb = hb;
+      th.maxrank = 0;
+      // halo points read by the tile
+      std::vector<int32_t> hp;
+      for (int32_t e : tile_elems[t])
+        for (int k = 0; k < npe; ++k) {
+          const int32_t g = l2g[static_cast<std::size_t>(e) * npe + k];
+          if (g >= 0 && owner[g] != t && tpi_stamp[g] != t) {
+            tpi_stamp[g] = t;
+            hp.push_back(perm[g]);
+          }
+        }
+      std::sort(hp.begin(), hp.end());
+      for (std::size_t q = 0; q < hp.size(); ++q) htp.push_back(hp[q]);
+      th.ntp = th.nc + static_cast<int32_t>(hp.size());
+      // tile point index of every point the tile touches
+      for (std::size_t q = 0; q < hp.size(); ++q) tpi[hp[q]] = th.nc + static_cast<int32_t>(q);
+      int32_t nh = 0;
+      for (int el = 0; el < th.ne; ++el) {
+        const int32_t e = tile_elems[t][el];
+        for (int k = 0; k < npe; ++k) {
+          const std::size_t s = static_cast<std::size_t>(e) * npe + k;
+          const int32_t g = l2g[s];
+          const int32_t ls = el * npe + k;
+          uint32_t dsc;
+          if (g >= 0) {
+            const int32_t pg = perm[g];
+            const int32_t p = owner[g] == t ? pg - th.cbeg : tpi[pg];
+            INSEM_REQUIRE(p >= 0 && p < 65536, INSEM_CUDA_ERR_UNSUPPORTED, "tile has too many points");
+            const uint32_t rank = owner[g] == t ? rank_of[s] : kSlotRankNone;
+            dsc = static_cast<uint32_t>(p) | (rank << kSlotRankShift);
+            if (owner[g] == t) {
+              th.maxrank = std::max<int32_t>(th.maxrank, static_cast<int32_t>(rank));
+            } else {
+              hpos_of_slot[s] = hb + nh++;
+              hslot.push_back(ls);
+            }
+          } else {
+            dsc = kSlotConstrained | (kSlotRankNone << kSlotRankShift);
+            cslot.push_back(ls);
+            cidx.push_back(static_cast<int32_t>(crow.size()));
+            crow.push_back(-1 - g);
+            hpos_of_slot[s] = hb + nh++;
+            hslot.push_back(ls);
+          }
+          desc[(static_cast<std::size_t>(e_running) + be + el) * npe + k] = dsc;
+        }
+      }
+      th.nhs = nh;
+      th.ncs = static_cast<int32_t>(cslot.size()) - th.cs_off;
+      hb += nh;
+      be += th.ne;
+    }
+    e_running += be;
+  }
+  n_hbuf = hb;
+  n_cslots = static_cast<int32_t>(crow.size());
+  tp_cap = 1;
+  for (const auto& th : hdr) tp_cap = std::max(tp_cap, th.ntp);
+
+  // 6. halo CSR and special records (device order of halo points)
+  std::vector<int32_t> hoff{0}, hpos, hspec(n_halo, -1), soff{0}, swhich, coff{0}, cidx2, aidx;
+  std::vector<float> hw, scoef;
+  std::vector<uint8_t> zm;
+  std::vector<int32_t> halo_orig(n_halo);
+  for (int32_t g = 0; g < ng; ++g)
+    if (owner[g] < 0) halo_orig[perm[g] - n_complete] = g;
+  for (int32_t h = 0; h < n_halo; ++h) {
+    const int32_t g = halo_orig[h];
+    for (int32_t s = t_off[g]; s < t_off[g + 1]; ++s) {
+      const int32_t pos = hpos_of_slot[t_slots[s]];
+      INSEM_REQUIRE(pos >= 0, INSEM_CUDA_ERR_INVALID, "halo contribution without a halo-buffer entry");
+      hpos.push_back(pos);
+      if (weighted) hw.push_back(static_cast<float>(t_w[s]));
+    }
+    hoff.push_back(static_cast<int32_t>(hpos.size()));
+    if (!special[g]) continue;
+    const int32_t rec = static_cast<int32_t>(aidx.size());
+    hspec[h] = rec;
+    if (auto it = sp.sources.find(g); it != sp.sources.end())
+      for (const auto& [s, cs] : it->second) {
+        swhich.push_back(s);
+        scoef.insert(scoef.end(), cs.begin(), cs.end());
+      }
+    soff.push_back(static_cast<int32_t>(swhich.size()));
+    if (auto it = sp.coupling.find(g); it != sp.coupling.end())
+      for (int32_t ci : it->second) cidx2.push_back(ci);
+    coff.push_back(static_cast<int32_t>(cidx2.size()));
+    auto ia = sp.absorbing.find(g);
+    aidx.push_back(ia == sp.absorbing.end() ? -1 : ia->second);
+    auto iz = sp.zero.find(g);
+    zm.push_back(iz == sp.zero.end() ? 0 : iz->second);
+  }
+
+  // 7. uploads
+  sdesc.upload(desc);
+  tiles.upload(hdr);
+  halo_tp.upload(htp.empty() ? std::vector<int32_t>{0} : htp);
+  hs_slot.upload(hslot.empty() ? std::vector<int32_t>{0} : hslot);
+  cs_slot.upload(cslot.empty() ? std::vector<int32_t>{0} : cslot);
+  cs_idx.upload(cidx.empty() ? std::vector<int32_t>{0} : cidx);
+  cs_row.upload(crow.empty() ? std::vector<int32_t>{0} : crow);
+  cval.resize(static_cast<std::size_t>(ncomp) * std::max(n_cslots, 1));
+  hbuf.resize(static_cast<std::size_t>(ncomp) * std::max(n_hbuf, 1));
+  h_off.upload(hoff);
+  h_pos.upload(hpos.empty() ? std::vector<int32_t>{0} : hpos);
+  if (weighted) h_w.upload(hw.empty() ? std::vector<float>{0.0f} : hw);
+  h_spec.upload(hspec.empty() ? std::vector<int32_t>{0} : hspec);
+  src_off.upload(soff);
+  src_which.upload(swhich.empty() ? std::vector<int32_t>{0} : swhich);
+  src_coef.upload(scoef.empty() ? std::vector<float>{0.0f} : scoef);
+  cpl_off.upload(coff);
+  cpl_idx.upload(cidx2.empty() ? std::vector<int32_t>{0} : cidx2);
+  abs_idx.upload(aidx.empty() ? std::vector<int32_t>{0} : aidx);
+  zero.upload(zm.empty() ? std::vector<uint8_t>{0} : zm);
+  abs_coef_d.upload(abs_coef_host.empty() ? std::vector<float>{0.0f} : abs_coef_host);
+  // constraint rows with device-numbered dofs (weights rounded as the gather does)
+  {
+    const auto ro = host_vec(d.dofs.row_offsets, static_cast<std::size_t>(d.dofs.n_rows) + 1);
+    const std::size_t nrd = ro.empty() ? 0 : static_cast<std::size_t>(ro.back());
+    auto rd = host_vec(d.dofs.row_dofs, nrd);
+    const auto rw = host_vec(d.dofs.row_weights, nrd);
+    for (auto& g : rd) g = perm[g];
+    rows_off.upload(ro.empty() ? std::vector<int32_t>{0} : ro);
+    rows_dofs.upload(rd.empty() ? std::vector<int32_t>{0} : rd);
+    rows_w.upload(rw.empty() ? std::vector<float>{0.0f} : std::vector<float>(rw.begin(), rw.end()));
+  }
+  // mass in device numbering
+  const auto mh = host_vec(d.mass, ng), imh = host_vec(d.inv_mass, ng);
+  host_mass.assign(ng, 0.0f);
+  std::vector<float> im(ng);
+  for (int32_t g = 0; g < ng; ++g) {
+    host_mass[perm[g]] = mh[g];
+    im[perm[g]] = imh[g];
+  }
+  mass.upload(host_mass);
+  inv_mass.upload(im);
+  const std::size_t nf = static_cast<std::size_t>(ncomp) * ng;
+  for (auto* buf : {&u0, &u1, &v, &a, &vn}) {
+    buf->resize(nf);
+    buf->zero();
+  }
+  // element data of every block in tile order
+  const int ngl = ngll;
+  for (int b = 0; b < d.n_blocks; ++b) {
+    const insem_cuda_block& src = d.blocks[b];
+    std::vector<int32_t> order;  // block-local positions in tile order
+    for (int t = blocks[b].tile0; t < blocks[b].tile0 + blocks[b].ntiles; ++t)
+      for (int32_t e : tile_elems[t]) order.push_back(epos[e]);
+    const std::size_t n = order.size();
+    const int mstride = src.kind == INSEM_RECT ? 3 : src.kind == INSEM_AFFINE ? 5 : 5 * npe;
+    std::vector<float> met(n * mstride), c0(n * npe), c1, wr, hp, rr;
+    std::vector<uint8_t> ax;
+    const bool el = medium == INSEM_ELASTIC;
+    if (el) c1.resize(n * npe);
+    const bool axi = src.kind == INSEM_AXISYM;
+    if (axi) {
+      wr.resize(n * npe);
+      hp.resize(n * npe);
+      rr.resize(n * npe);
+      ax.resize(n);
+    }
+    for (std::size_t q = 0; q < n; ++q) {
+      const std::size_t o = order[q];
+      if (src.kind == INSEM_RECT || src.kind == INSEM_AFFINE) {
+        for (int k = 0; k < mstride; ++k) met[q * mstride + k] = src.metric[o * mstride + k];
+      } else {
+        for (int k = 0; k < npe; ++k)
+          for (int c = 0; c < 5; ++c) met[(q * 5 + c) * npe + k] = src.metric[(o * npe + k) * 5 + c];
+      }
+      for (int k = 0; k < npe; ++k) {
+        c0[q * npe + k] = src.coef0[o * npe + k];
+        if (el) c1[q * npe + k] = src.coef1[o * npe + k];
+        if (axi) {
+          wr[q * npe + k] = src.wr[o * npe + k];
+          hp[q * npe + k] = src.hoop[o * npe + k];
+          rr[q * npe + k] = src.r[o * npe + k];
+        }
+      }
+      if (axi) ax[q] = src.axial[o];
+    }
+    (void)ngl;
+    blocks[b].metric.upload(met);
+    blocks[b].coef0.upload(c0);
+    if (el) blocks[b].coef1.upload(c1);
+    if (axi) {
+      blocks[b].wr.upload(wr);
+      blocks[b].hoop.upload(hp);
+      blocks[b].r.upload(rr);
+      blocks[b].axial.upload(ax);
+    }
+  }
+}
+
+}  // namespace insem_b200

@@ -1,0 +1,135 @@
+// Host side of the tiled fused step: tiling, device numbering and launches.
+#pragma once
+
+#include <map>
+#include <vector>
+
+#include "device_data.cuh"
+#include "tiled.cuh"
+
+namespace insem_b200 {
+
+// Per-point special terms of one domain, in the reference's point numbering.
+struct SpecialTerms {
+  std::map<int32_t, std::vector<std::pair<int32_t, std::vector<float>>>> sources;  // point -> (source, coef[ncomp])
+  std::map<int32_t, std::vector<int32_t>> coupling;                               // point -> coupling entries
+  std::map<int32_t, int32_t> absorbing;                                           // point -> Stacey index
+  std::map<int32_t, uint8_t> zero;                                                // point -> zeroed components
+  std::vector<int32_t> receivers;                                                 // points read by receivers
+};
+
+// One domain of the tiled path.
+class TiledDomain {
+ public:
+  // Builds tiles of at most `te` elements per block and the device numbering.
+  void build(const insem_cuda_domain& d, int ngll, int te, const SpecialTerms& sp, const std::vector<float>& abs_coef);
+
+  int medium = 0, ncomp = 1, m = 0, ng = 0, npe = 0, n_elements = 0;
+  int n_complete = 0, n_halo = 0, n_tiles = 0, tp_cap = 0, n_hbuf = 0, n_cslots = 0;
+  bool weighted = false;
+  std::vector<int32_t> perm;  // reference point -> device point
+  struct BlockTiles {
+    int kind = 0, m = 0, tile0 = 0, ntiles = 0, n = 0, e_off = 0;
+    DeviceBuffer<float> metric, coef0, coef1, wr, hoop, r;
+    DeviceBuffer<uint8_t> axial;
+    BlockDev view() const;
+  };
+  std::vector<BlockTiles> blocks;
+  // device data
+  DeviceBuffer<uint32_t> sdesc;
+  DeviceBuffer<TileHdr> tiles;
+  DeviceBuffer<int32_t> halo_tp, hs_slot, cs_slot, cs_idx, cs_row;
+  DeviceBuffer<float> cval, hbuf, mass, inv_mass;
+  DeviceBuffer<float> u0, u1, v, a, vn;
+  DeviceBuffer<int32_t> h_off, h_pos, h_spec, src_off, src_which, cpl_off, cpl_idx, abs_idx;
+  DeviceBuffer<float> h_w, src_coef, abs_coef_d;
+  DeviceBuffer<uint8_t> zero;
+  DeviceBuffer<int32_t> rows_off, rows_dofs;  // constraint rows in device numbering
+  DeviceBuffer<float> rows_w;
+  RowsDev rows() const { return {rows_off.get(), rows_dofs.get(), rows_w.get()}; }
+  std::vector<float> host_mass;
+
+  TiledDev view(int parity) const;  // parity 0: u0 current, u1 next
+  HaloDev halo_view() const;
+  float* u_cur(int parity) { return parity ? u1.get() : u0.get(); }
+};
+
+// Launchers, instantiated per ngll in tiled_ng.cu.
+struct TileLaunch {
+  const TiledDomain* dom = nullptr;
+  int block = 0;
+  int parity = 0;
+  StepScalars sc{};
+  const StepState* st = nullptr;
+  double* epartial = nullptr;
+  bool elastic = false;
+  cudaStream_t stream = nullptr;
+};
+void launch_tiles_ng2(const TileLaunch&);
+void launch_tiles_ng3(const TileLaunch&);
+void launch_tiles_ng4(const TileLaunch&);
+void launch_tiles_ng5(const TileLaunch&);
+void launch_tiles_ng6(const TileLaunch&);
+void launch_tiles_ng7(const TileLaunch&);
+void launch_tiles_ng8(const TileLaunch&);
+void launch_tiles_ng9(const TileLaunch&);
+void launch_tiles(int ngll, const TileLaunch& a);
+int tile_elements(int ngll);  // TileCfg<NG>::TE
+// Uploads the GLL / GLJ basis of one ngll to constant memory (must agree with earlier uploads).
+void set_constant_basis(int ngll, const std::vector<float>& D, const std::vector<float>& Dj,
+                        const std::vector<float>& w2);
+
+template <int NG>
+void launch_tiles_cfg(const TileLaunch& a) {
+  const TiledDomain& d = *a.dom;
+  const auto& b = d.blocks[a.block];
+  if (b.ntiles == 0) return;
+  auto go = [&](auto kernel, int nc) {
+    const size_t smem = (nc == 1)   ? TileSmem<NG, 1>::bytes(d.tp_cap)
+                        : (nc == 2) ? TileSmem<NG, 2>::bytes(d.tp_cap)
+                                    : TileSmem<NG, 3>::bytes(d.tp_cap);
+    // Opt in to this launch's dynamic shared memory (outside stream capture;
+    // the first launch of every tile kernel happens in the uncaptured initial step).
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_CHECK(cudaStreamIsCapturing(a.stream, &cap));
+    if (cap == cudaStreamCaptureStatusNone)
+      CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    INSEM_REQUIRE(smem <= 227 * 1024, INSEM_CUDA_ERR_UNSUPPORTED, "tile needs too much shared memory");
+    TiledDev td = d.view(a.parity);
+    td.sdesc += static_cast<size_t>(b.e_off) * NG * NG;
+    kernel<<<b.ntiles, TileCfg<NG>::THREADS, smem, a.stream>>>(b.view(), td, a.sc, a.st, a.epartial, b.tile0,
+                                                                d.tp_cap);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess)
+      throw Error(INSEM_CUDA_ERR_CUDA, "tile kernel launch (ngll " + std::to_string(NG) + ", kind " +
+                                           std::to_string(b.kind) + ", tiles " + std::to_string(b.ntiles) +
+                                           ", threads " + std::to_string(TileCfg<NG>::THREADS) + ", smem " +
+                                           std::to_string(smem) + "): " + cudaGetErrorString(err));
+  };
+  if (b.kind == INSEM_AXISYM) {
+    if (b.m == 1) {
+      if (a.elastic) go(tile_step_kernel<NG, INSEM_AXISYM, true, 1>, 3);
+      else go(tile_step_kernel<NG, INSEM_AXISYM, false, 1>, 1);
+    } else {
+      if (a.elastic) go(tile_step_kernel<NG, INSEM_AXISYM, true, 0>, 2);
+      else go(tile_step_kernel<NG, INSEM_AXISYM, false, 0>, 1);
+    }
+    return;
+  }
+  switch (b.kind) {
+    case INSEM_RECT:
+      if (a.elastic) go(tile_step_kernel<NG, INSEM_RECT, true, 0>, 2);
+      else go(tile_step_kernel<NG, INSEM_RECT, false, 0>, 1);
+      break;
+    case INSEM_AFFINE:
+      if (a.elastic) go(tile_step_kernel<NG, INSEM_AFFINE, true, 0>, 2);
+      else go(tile_step_kernel<NG, INSEM_AFFINE, false, 0>, 1);
+      break;
+    default:
+      if (a.elastic) go(tile_step_kernel<NG, INSEM_CURVED, true, 0>, 2);
+      else go(tile_step_kernel<NG, INSEM_CURVED, false, 0>, 1);
+      break;
+  }
+}
+
+}  // namespace insem_b200

@@ -78,11 +78,12 @@ def run_case(pkg, z, **opts):
     return prob, s
 
 
+@pytest.mark.parametrize("path", [0, 1], ids=["tiled", "plain"])
 @pytest.mark.parametrize("graphs", [True, False])
 @pytest.mark.parametrize("case", RUN_CASES)
-def test_run_bitwise(pkg, case, graphs):
+def test_run_bitwise(pkg, case, graphs, path):
     z = golden(case)
-    prob, s = run_case(pkg, z, use_graphs=graphs)
+    prob, s = run_case(pkg, z, use_graphs=graphs, path=path)
     with s:
         assert s.step == prob.n_steps
         assert np.array_equal(s.times, z["run.times"])
@@ -129,7 +130,7 @@ def test_streamed_advance_matches_traces(pkg, case):
         rows = np.zeros((n // prob.record_every + 1, s.n_columns))
         got = s.advance_streamed(n, amp, rows)
         assert s.step == prob.n_steps
-        assert s.kernels_per_step > 5
+        assert s.kernels_per_step >= 3
     cols = []
     for name, q in prob.trace_list():
         cols.append(z[f"run.trace.{name}.{q}"])
