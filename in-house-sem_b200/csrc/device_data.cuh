@@ -34,6 +34,58 @@ struct DeviceBasis {
   BasisDev view() const { return {D.get(), Dj.get(), w2.get()}; }
 };
 
+// A block's element data in the padded device layout (element_ops.cuh),
+// elements taken in `order` (block-local positions): metric Rect 4 / Affine 8
+// floats per element, per-point arrays CS = npe rounded up to 4 per element,
+// per-point metric [element][component][CS] (transposed from the reference's
+// [element][point][5]).
+struct PackedBlock {
+  std::vector<float> metric, coef0, coef1, wr, hoop, r;
+  std::vector<uint8_t> axial;
+};
+
+inline PackedBlock pack_block(const insem_cuda_block& b, int npe, int medium, const std::vector<int32_t>& order) {
+  PackedBlock pk;
+  const std::size_t n = order.size(), cs = point_stride_rt(npe);
+  const std::size_t ms = metric_stride_rt(b.kind, npe);
+  pk.metric.assign(n * ms, 0.0f);
+  pk.coef0.assign(n * cs, 0.0f);
+  const bool el = medium == INSEM_ELASTIC, axi = b.kind == INSEM_AXISYM;
+  if (el) pk.coef1.assign(n * cs, 0.0f);
+  if (axi) {
+    pk.wr.assign(n * cs, 0.0f);
+    pk.hoop.assign(n * cs, 0.0f);
+    pk.r.assign(n * cs, 0.0f);
+    pk.axial.assign(n, 0);
+  }
+  INSEM_REQUIRE(b.n_elements == 0 || (b.metric && b.coef0), INSEM_CUDA_ERR_INVALID, "block arrays missing");
+  INSEM_REQUIRE(!el || b.n_elements == 0 || b.coef1, INSEM_CUDA_ERR_INVALID, "elastic block needs coef1");
+  INSEM_REQUIRE(!axi || b.n_elements == 0 || (b.wr && b.hoop && b.r && b.axial), INSEM_CUDA_ERR_INVALID,
+                "axisymmetric block needs wr, hoop, r and axial");
+  for (std::size_t q = 0; q < n; ++q) {
+    const std::size_t o = static_cast<std::size_t>(order[q]);
+    INSEM_REQUIRE(o < static_cast<std::size_t>(b.n_elements), INSEM_CUDA_ERR_INVALID, "element order out of range");
+    if (b.kind == INSEM_RECT || b.kind == INSEM_AFFINE) {
+      const int src = b.kind == INSEM_RECT ? 3 : 5;
+      for (int k = 0; k < src; ++k) pk.metric[q * ms + k] = b.metric[o * src + k];
+    } else {
+      for (int k = 0; k < npe; ++k)
+        for (int c = 0; c < 5; ++c) pk.metric[(q * 5 + c) * cs + k] = b.metric[(o * npe + k) * 5 + c];
+    }
+    for (int k = 0; k < npe; ++k) {
+      pk.coef0[q * cs + k] = b.coef0[o * npe + k];
+      if (el) pk.coef1[q * cs + k] = b.coef1[o * npe + k];
+      if (axi) {
+        pk.wr[q * cs + k] = b.wr[o * npe + k];
+        pk.hoop[q * cs + k] = b.hoop[o * npe + k];
+        pk.r[q * cs + k] = b.r[o * npe + k];
+      }
+    }
+    if (axi) pk.axial[q] = b.axial[o];
+  }
+  return pk;
+}
+
 struct DeviceBlock {
   int kind = 0, m = 0, n = 0;
   DeviceBuffer<int32_t> elements;
@@ -51,29 +103,21 @@ struct DeviceBlock {
     INSEM_REQUIRE(m == 0 || (m == 1 && kind == INSEM_AXISYM), INSEM_CUDA_ERR_UNSUPPORTED,
                   "no kernel for azimuthal order " + std::to_string(m) + " on non-axisymmetric elements");
     INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative block size");
-    const std::size_t npe = static_cast<std::size_t>(ngll) * ngll;
+    const int npe = ngll * ngll;
     host_elements = host_vec(b.elements, n);
     elements.upload(host_elements);
-    if (kind == INSEM_RECT || kind == INSEM_AFFINE) {
-      metric.upload(host_vec(b.metric, static_cast<std::size_t>(n) * (kind == INSEM_RECT ? 3 : 5)));
-    } else {
-      // [n][npe][5] -> [n][5][npe]
-      const auto src = host_vec(b.metric, static_cast<std::size_t>(n) * npe * 5);
-      std::vector<float> dst(src.size());
-      for (std::size_t e = 0; e < static_cast<std::size_t>(n); ++e)
-        for (std::size_t k = 0; k < npe; ++k)
-          for (std::size_t q = 0; q < 5; ++q) dst[(e * 5 + q) * npe + k] = src[(e * npe + k) * 5 + q];
-      metric.upload(dst);
-    }
-    coef0.upload(host_vec(b.coef0, n * npe));
-    if (medium == INSEM_ELASTIC) coef1.upload(host_vec(b.coef1, n * npe));
+    std::vector<int32_t> order(n);
+    for (int q = 0; q < n; ++q) order[q] = q;
+    PackedBlock pk = pack_block(b, npe, medium, order);
+    metric.upload(pk.metric);
+    coef0.upload(pk.coef0);
+    if (medium == INSEM_ELASTIC) coef1.upload(pk.coef1);
     if (kind == INSEM_AXISYM) {
-      wr.upload(host_vec(b.wr, n * npe));
-      hoop.upload(host_vec(b.hoop, n * npe));
-      r.upload(host_vec(b.r, n * npe));
-      const auto ax = host_vec(b.axial, n);
-      for (auto a : ax) any_axial |= a != 0;
-      axial.upload(ax);
+      wr.upload(pk.wr);
+      hoop.upload(pk.hoop);
+      r.upload(pk.r);
+      for (auto a : pk.axial) any_axial |= a != 0;
+      axial.upload(pk.axial);
     }
   }
   BlockDev view() const {

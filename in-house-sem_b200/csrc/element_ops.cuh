@@ -126,31 +126,46 @@ __device__ __forceinline__ void el_stress(float lambda, float mu, float ux_x, fl
   sxz = fmul(mu, fadd(ux_z, uz_x));
 }
 
+// Padded strides of the device layout (16-byte multiples, so that every
+// element's data can be moved with bulk copies):
+//   per-point arrays: CS = npe rounded up to 4 floats per element (and per
+//                     metric component);
+//   metric: Rect 4 floats, Affine 8 floats, Curved / Axisym 5 * CS floats.
+template <int NPE>
+constexpr int point_stride() {
+  return (NPE + 3) & ~3;
+}
+inline int point_stride_rt(int npe) { return (npe + 3) & ~3; }
+inline int metric_stride_rt(int kind, int npe) {
+  return kind == INSEM_RECT ? 4 : kind == INSEM_AFFINE ? 8 : 5 * point_stride_rt(npe);
+}
+
 // Metric of block element b at point k in the device layout.
 template <int KIND, int NPE>
 __device__ __forceinline__ void load_metric(const float* metric, int b, int k, float& xi_x, float& xi_z,
                                             float& eta_x, float& eta_z, float& jac) {
+  constexpr int CS = point_stride<NPE>();
   if constexpr (KIND == INSEM_RECT) {
-    const float* m = metric + static_cast<size_t>(b) * 3;
+    const float* m = metric + static_cast<size_t>(b) * 4;
     xi_x = m[0];
     xi_z = 0.0f;
     eta_x = 0.0f;
     eta_z = m[1];
     jac = m[2];
   } else if constexpr (KIND == INSEM_AFFINE) {
-    const float* m = metric + static_cast<size_t>(b) * 5;
+    const float* m = metric + static_cast<size_t>(b) * 8;
     xi_x = m[0];
     xi_z = m[1];
     eta_x = m[2];
     eta_z = m[3];
     jac = m[4];
   } else {
-    const float* m = metric + static_cast<size_t>(b) * 5 * NPE + k;
+    const float* m = metric + static_cast<size_t>(b) * 5 * CS + k;
     xi_x = m[0];
-    xi_z = m[NPE];
-    eta_x = m[2 * NPE];
-    eta_z = m[3 * NPE];
-    jac = m[4 * NPE];
+    xi_z = m[CS];
+    eta_x = m[2 * CS];
+    eta_z = m[3 * CS];
+    jac = m[4 * CS];
   }
 }
 
@@ -166,10 +181,11 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
                                            float* fy, float* direct, float* gx0, float* gy0, float* gx1,
                                            float* gy1, float w2k) {
   constexpr int NPE = NG * NG;
+  constexpr int CS = point_stride<NPE>();
   if constexpr (KIND != INSEM_AXISYM) {
     float xi_x, xi_z, eta_x, eta_z, jac;
     load_metric<KIND, NPE>(blk.metric, bb, kpt, xi_x, xi_z, eta_x, eta_z, jac);
-    const size_t p = static_cast<size_t>(bb) * NPE + kpt;
+    const size_t p = static_cast<size_t>(bb) * CS + kpt;
     if constexpr (ELASTIC) {
       // elastic_kernel (kernels.cpp:64-120)
       float ux_x, ux_z, uz_x, uz_z;
@@ -207,9 +223,9 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
       }
     }
   } else {
-    const size_t p = static_cast<size_t>(bb) * NPE + kpt;
-    const float* mt = blk.metric + static_cast<size_t>(bb) * 5 * NPE + kpt;
-    const float xi_r = mt[0], xi_z = mt[NPE], eta_r = mt[2 * NPE], eta_z = mt[3 * NPE];
+    const size_t p = static_cast<size_t>(bb) * CS + kpt;
+    const float* mt = blk.metric + static_cast<size_t>(bb) * 5 * CS + kpt;
+    const float xi_r = mt[0], xi_z = mt[CS], eta_r = mt[2 * CS], eta_z = mt[3 * CS];
     const bool axis_pt = axial && i == 0;
     if constexpr (ELASTIC && M == 0) {
       // elastic_axisym_kernel (kernels.cpp:206-263)

@@ -570,14 +570,15 @@ void Solver::set_state(int32_t medium, const double* u_in, const double* v_in) {
   CUDA_CHECK(cudaMemcpy(d.v.get(), fv.data(), n * sizeof(float), cudaMemcpyHostToDevice));
   if (tiled) {
     TiledDomain& t = tdom[di];
-    std::vector<float> pu(n), pv(n);
+    const std::size_t nd = static_cast<std::size_t>(d.ncomp) * t.ng;
+    std::vector<float> pu(nd, 0.0f), pv(nd, 0.0f);
     for (int c = 0; c < d.ncomp; ++c)
       for (int32_t g = 0; g < d.ng; ++g) {
-        pu[static_cast<std::size_t>(c) * d.ng + t.perm[g]] = fu[static_cast<std::size_t>(c) * d.ng + g];
-        pv[static_cast<std::size_t>(c) * d.ng + t.perm[g]] = fv[static_cast<std::size_t>(c) * d.ng + g];
+        pu[static_cast<std::size_t>(c) * t.ng + t.perm[g]] = fu[static_cast<std::size_t>(c) * d.ng + g];
+        pv[static_cast<std::size_t>(c) * t.ng + t.perm[g]] = fv[static_cast<std::size_t>(c) * d.ng + g];
       }
-    CUDA_CHECK(cudaMemcpy(t.u_cur(parity), pu.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-    CUDA_CHECK(cudaMemcpy(t.v.get(), pv.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpy(t.u_cur(parity), pu.data(), nd * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpy(t.v.get(), pv.data(), nd * sizeof(float), cudaMemcpyHostToDevice));
   }
 }
 
@@ -711,11 +712,11 @@ void Solver::copy_state(int32_t di, double* u_out, double* v_out, double* a_out)
     TiledDomain& t = tdom[di];
     auto conv = [&](const float* dev, double* out) {
       if (!out) return;
-      std::vector<float> h(static_cast<std::size_t>(d.ncomp) * d.ng);
+      std::vector<float> h(static_cast<std::size_t>(d.ncomp) * t.ng);
       CUDA_CHECK(cudaMemcpy(h.data(), dev, h.size() * sizeof(float), cudaMemcpyDeviceToHost));
       for (int c = 0; c < d.ncomp; ++c)
         for (int32_t g = 0; g < d.ng; ++g)
-          out[static_cast<std::size_t>(c) * d.ng + g] = h[static_cast<std::size_t>(c) * d.ng + t.perm[g]];
+          out[static_cast<std::size_t>(c) * d.ng + g] = h[static_cast<std::size_t>(c) * t.ng + t.perm[g]];
     };
     conv(t.u_cur(parity), u_out);
     conv(t.v.get(), v_out);
@@ -994,11 +995,11 @@ void Solver::advance_tiled(int32_t n, const float* amp_in, double* rows_out, int
   CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
   last_ms = ms;
   *n_rows = rows;
-  if (opts.check_finite && !streamed) {
-    StepState hs;
-    CUDA_CHECK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
+  StepState hs;
+  CUDA_CHECK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
+  INSEM_REQUIRE(!hs.error, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
+  if (opts.check_finite && !streamed)
     INSEM_REQUIRE(!hs.nonfinite, INSEM_CUDA_ERR_NONFINITE, "the solution contains NaN or Inf (unstable time step?)");
-  }
 }
 
 }  // namespace insem_b200

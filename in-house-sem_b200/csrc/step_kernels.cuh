@@ -19,7 +19,7 @@ struct StepState {
   int32_t step;           // current step index (after the predictor's increment)
   int32_t nonfinite;      // set when a NaN/Inf was found
   int32_t mode;           // tiled path: 0 normal, 1 final (state complete), 2 initial
-  int32_t pad;
+  int32_t error;          // a bounded device-side wait gave up
   double kin_c;           // dt^2 / 8 of the kinetic energy (solver.cpp:903)
 };
 

@@ -94,18 +94,101 @@ struct TileCfg {
 
 __device__ __forceinline__ float cbasis(int ng, int which, int idx) { return c_basis[ng - 2][which][idx]; }
 
-// Shared-memory layout of one tile CTA (dynamic; TP = tile point capacity).
-template <int NG, int NC>
-struct TileSmem {
-  using Cfg = TileCfg<NG>;
-  static constexpr int ROWS_PER_EL = NC * NG;                     // rows of one element
-  static constexpr int EL_FLOATS = ROWS_PER_EL * Cfg::ROW;
-  static size_t bytes(int tp) {
-    return sizeof(float) * (2 * static_cast<size_t>(NC) * tp + 2 * static_cast<size_t>(Cfg::TE) * EL_FLOATS +
-                            static_cast<size_t>(Cfg::TE) * 4 * 16);
+
+// ------------------------------------------------------- bulk-copy helpers
+// One mbarrier per CTA tracks the tile's bulk copies (cp.async.bulk, the
+// non-tensor TMA path): thread 0 announces the byte count and issues the
+// copies; every thread waits on the barrier's phase 0.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls (each poll may suspend the
+// thread for a hardware-defined interval) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+constexpr uint32_t kBulkWaitLimit = 1u << 22;
+
+// Shared-memory layout of one tile CTA, byte offsets (16-byte aligned).
+// Per-tile data arrives by bulk copies: element data (metric, coefficients,
+// axisymmetric weights), slot descriptors, and the complete points' u, v
+// and inverse mass; halo tile points are gathered by the threads into the u
+// region after the complete points (at index roundup(nc, 4) on).
+struct TileLayout {
+  uint32_t bar, metric, coef0, coef1, wr, hoop, r, desc, u, v, im, tf, su, sfx, ax, total;
+  int32_t tp_cap, nc_cap, ms, cs, row;
+
+  __host__ __device__ static uint32_t up16(uint32_t x) { return (x + 15u) & ~15u; }
+  __host__ __device__ static TileLayout make(int ng, int nc, int kind, bool elastic, int te, int tp_cap, int nc_cap) {
+    TileLayout L{};
+    const int npe = ng * ng;
+    L.cs = (npe + 3) & ~3;
+    L.ms = kind == INSEM_RECT ? 4 : kind == INSEM_AFFINE ? 8 : 5 * L.cs;
+    L.row = (ng + 1) & ~1;
+    L.tp_cap = tp_cap;
+    L.nc_cap = nc_cap;
+    const bool axi = kind == INSEM_AXISYM;
+    uint32_t o = 0;
+    L.bar = o;
+    o = up16(o + 8);
+    L.metric = o;
+    o = up16(o + 4u * te * L.ms);
+    L.coef0 = o;
+    o = up16(o + 4u * te * L.cs);
+    L.coef1 = o;
+    if (elastic) o = up16(o + 4u * te * L.cs);
+    L.wr = o;
+    if (axi) o = up16(o + 4u * te * L.cs);
+    L.hoop = o;
+    if (axi) o = up16(o + 4u * te * L.cs);
+    L.r = o;
+    if (axi) o = up16(o + 4u * te * L.cs);
+    L.desc = o;
+    o = up16(o + 4u * te * L.cs);
+    L.u = o;
+    o = up16(o + 4u * nc * tp_cap);
+    L.v = o;
+    o = up16(o + 4u * nc * nc_cap);
+    L.im = o;
+    o = up16(o + 4u * nc_cap);
+    L.tf = o;
+    o = up16(o + 4u * nc * tp_cap);
+    L.su = o;
+    o = up16(o + 4u * te * nc * ng * L.row);
+    L.sfx = o;
+    o = up16(o + 4u * te * nc * ng * L.row);
+    L.ax = o;
+    if (axi) o = up16(o + 4u * te * 64);
+    L.total = o;
+    return L;
   }
 };
 
+// Mode-dependent completion of a point (solver.cpp:924-944 fused):
 // Mode-dependent completion of a point (solver.cpp:924-944 fused):
 //   normal: v = v_half + dt/2 a; u' = u + dt v + dt^2/2 a; v' = v + dt/2 a
 //   final:  v = v_half + dt/2 a; u' = u                      (state complete)
@@ -156,41 +239,93 @@ static __global__ void predictor_inplace_kernel(float* __restrict__ u, float* __
 
 template <int NG, int KIND, bool EL, int M>
 static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
-    tile_step_kernel(BlockDev blk, TiledDev td, StepScalars sc, const StepState* __restrict__ st,
-                     double* __restrict__ epartial, int32_t tile0, int32_t tp_cap) {
+    tile_step_kernel(BlockDev blk, TiledDev td, StepScalars sc, StepState* __restrict__ st,
+                     double* __restrict__ epartial, int32_t tile0, TileLayout L) {
   using Cfg = TileCfg<NG>;
   using CE = ElemCfg<NG, KIND, EL, M>;
   constexpr int NC = CE::NC;
   constexpr int NPE = NG * NG;
+  constexpr int CS = point_stride<NPE>();
   constexpr int ROW = Cfg::ROW;
   constexpr bool AXI = KIND == INSEM_AXISYM;
-  extern __shared__ __align__(16) float smem[];
-  float* tu = smem;                                 // [NC][tp_cap]
-  float* tf = tu + NC * tp_cap;                     // [NC][tp_cap]
-  float* su = tf + NC * tp_cap;                     // [TE][NC][NG][ROW] field rows, later staging
-  float* sfx = su + Cfg::TE * NC * NG * ROW;        // [TE][NC][NG][ROW] f_xi rows
-  float* sax = sfx + Cfg::TE * NC * NG * ROW;       // [TE][4][16] axis terms (gx0, gy0, gx1, gy1)
+  constexpr int MS = KIND == INSEM_RECT ? 4 : KIND == INSEM_AFFINE ? 8 : 5 * CS;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + L.bar);
+  float* s_metric = reinterpret_cast<float*>(smem_raw + L.metric);
+  float* s_coef0 = reinterpret_cast<float*>(smem_raw + L.coef0);
+  float* s_coef1 = reinterpret_cast<float*>(smem_raw + L.coef1);
+  float* s_wr = reinterpret_cast<float*>(smem_raw + L.wr);
+  float* s_hoop = reinterpret_cast<float*>(smem_raw + L.hoop);
+  float* s_r = reinterpret_cast<float*>(smem_raw + L.r);
+  uint32_t* s_desc = reinterpret_cast<uint32_t*>(smem_raw + L.desc);
+  float* tu = reinterpret_cast<float*>(smem_raw + L.u);    // [NC][tp_cap]
+  float* s_v = reinterpret_cast<float*>(smem_raw + L.v);   // [NC][nc_cap]
+  float* s_im = reinterpret_cast<float*>(smem_raw + L.im); // [nc_cap]
+  float* tf = reinterpret_cast<float*>(smem_raw + L.tf);   // [NC][tp_cap]
+  float* su = reinterpret_cast<float*>(smem_raw + L.su);   // [TE][NC][NG][ROW] field rows, later staging
+  float* sfx = reinterpret_cast<float*>(smem_raw + L.sfx); // [TE][NC][NG][ROW] f_xi rows
+  float* sax = reinterpret_cast<float*>(smem_raw + L.ax);  // [TE][4][16] axis terms
+  const int tp_cap = L.tp_cap, nc_cap = L.nc_cap;
 
   const TileHdr th = td.tiles[tile0 + blockIdx.x];
   const int tid = threadIdx.x;
   const int mode = st->mode;
   const int32_t step = st->step;
   const bool energy = (mode == kModeInit) ? (sc.energy_every > 0) : (sc.energy_every > 0 && step % sc.energy_every == 0);
+  const int nc4 = (th.nc + 3) & ~3;
 
-  // 1. tile points: complete range, then halo points the tile reads
-  for (int t = tid; t < th.ntp; t += Cfg::THREADS) {
-    const int32_t g = t < th.nc ? th.cbeg + t : td.halo_tp[th.hl_off + t - th.nc];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) tu[c * tp_cap + t] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
-  }
+  // 1. bulk copies of the tile's element data, slot descriptors and complete points
+  if (tid == 0) mbar_init(bar, 1);
   __syncthreads();
+  if (tid == 0) {
+    const uint32_t eb = 4u * th.ne;
+    uint32_t total = eb * MS + eb * CS * (1 + (EL ? 1 : 0) + (AXI ? 3 : 0)) + eb * CS;
+    if (nc4 > 0) total += 4u * nc4 * (2 * NC + 1);
+    mbar_expect_tx(bar, total);
+    bulk_load(s_metric, blk.metric + static_cast<size_t>(th.be0) * MS, eb * MS, bar);
+    bulk_load(s_coef0, blk.coef0 + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
+    if constexpr (EL) bulk_load(s_coef1, blk.coef1 + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
+    if constexpr (AXI) {
+      bulk_load(s_wr, blk.wr + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
+      bulk_load(s_hoop, blk.hoop + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
+      bulk_load(s_r, blk.r + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
+    }
+    bulk_load(s_desc, td.sdesc + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
+    if (nc4 > 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        bulk_load(tu + c * tp_cap, td.u_cur + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar);
+        bulk_load(s_v + c * nc_cap, td.v + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar);
+      }
+      bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar);
+    }
+  }
+  // halo tile points, gathered while the bulk copies are in flight
+  for (int t = tid; t < th.ntp - th.nc; t += Cfg::THREADS) {
+    const int32_t g = td.halo_tp[th.hl_off + t];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) tu[c * tp_cap + nc4 + t] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
+  }
+  const bool arrived = mbar_wait_bounded(bar, 0, kBulkWaitLimit);
+  if (__syncthreads_or(!arrived)) {
+    if (tid == 0) atomicExch(&st->error, 1);
+    return;
+  }
+
+  // element data now in shared memory, indexed by the tile-local element
+  BlockDev lb = blk;
+  lb.metric = s_metric;
+  lb.coef0 = s_coef0;
+  lb.coef1 = s_coef1;
+  lb.wr = s_wr;
+  lb.hoop = s_hoop;
+  lb.r = s_r;
 
   const int el = tid / NG;
   const int i = tid - el * NG;
   const bool active = el < th.ne;
-  const int bb = th.be0 + el;                           // block-local element (tile order)
-  const uint32_t* desc = td.sdesc + static_cast<size_t>(bb) * NPE;
-  float* urow = su + el * (NC * NG * ROW);              // this element's rows
+  const uint32_t* desc = s_desc + el * CS;
+  float* urow = su + el * (NC * NG * ROW);
   float* frow = sfx + el * (NC * NG * ROW);
   float* ax = sax + el * 64;
 
@@ -219,7 +354,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   __syncthreads();
 
   // 3. derivatives and fluxes, one column per thread
-  const bool axial = AXI && active && blk.axial[bb] != 0;
+  const bool axial = AXI && active && blk.axial[th.be0 + el] != 0;
   float dxr[NG], dxc[NG], w2c[NG];  // Dx row i, Dx column i, w_i w_j
 #pragma unroll
   for (int l = 0; l < NG; ++l) {
@@ -252,7 +387,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
       float fx[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
-      point_flux<NG, KIND, EL, M>(blk, bb, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
+      point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
                                   w2c[j]);
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
@@ -335,7 +470,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   double kin = 0.0, pot = 0.0;
   for (int t = tid; t < th.nc; t += Cfg::THREADS) {
     const int32_t g = th.cbeg + t;
-    const float im = td.inv_mass[g];
+    const float im = s_im[t];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       const size_t gi = static_cast<size_t>(c) * td.ng + g;
@@ -343,7 +478,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
       const float a = fmul(f, im);
       const float u = tu[c * tp_cap + t];
       float u_out, v_state, v_n;
-      complete_point(mode, sc, u, td.v[gi], a, u_out, v_state, v_n);
+      complete_point(mode, sc, u, s_v[c * nc_cap + t], a, u_out, v_state, v_n);
       td.u_nxt[gi] = u_out;
       td.v[gi] = v_state;
       if (mode != kModeNormal) td.a[gi] = a;
@@ -380,7 +515,6 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
     }
   }
 }
-
 
 // ------------------------------------------------------------ halo kernel
 // Special-point records of a domain's halo points.

@@ -145,7 +145,8 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
   medium = d.medium;
   ncomp = d.ncomp;
   m = d.azimuthal_order;
-  ng = d.dofs.n_global;
+  ng = d.dofs.n_global;  // reference count while building; the padded stride at the end
+  ng_ref = ng;
   npe = ngll * ngll;
   n_elements = d.dofs.n_elements;
   const std::size_t n_slots = static_cast<std::size_t>(n_elements) * npe;
@@ -235,16 +236,28 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
   std::vector<int32_t> count(n_tiles + 1, 0);
   for (int32_t g = 0; g < ng; ++g)
     if (owner[g] >= 0) ++count[owner[g] + 1];
+  // every tile's complete range starts on a multiple of 4 points (16 bytes)
+  // so it can be moved by bulk copies; the gaps are unused padding points
+  auto up4 = [](int32_t x) { return (x + 3) & ~3; };
   std::vector<int32_t> cbeg(n_tiles + 1, 0);
-  for (int t = 0; t < n_tiles; ++t) cbeg[t + 1] = cbeg[t] + count[t + 1];
+  for (int t = 0; t < n_tiles; ++t) cbeg[t + 1] = up4(cbeg[t] + count[t + 1]);
   n_complete = cbeg[n_tiles];
   perm.assign(ng, -1);
+  int32_t n_halo_pts = 0;
   {
     std::vector<int32_t> fill(cbeg.begin(), cbeg.end() - 1);
     int32_t h = n_complete;
-    for (int32_t g = 0; g < ng; ++g) perm[g] = owner[g] >= 0 ? fill[owner[g]]++ : h++;
+    for (int32_t g = 0; g < ng; ++g) {
+      if (owner[g] >= 0) perm[g] = fill[owner[g]]++;
+      else {
+        perm[g] = h++;
+        ++n_halo_pts;
+      }
+    }
   }
-  n_halo = ng - n_complete;
+  n_halo = n_halo_pts;
+  const int32_t ng_dev = std::max(up4(n_complete + n_halo), 4);
+  const int cs = point_stride_rt(npe);
 
   // 4. ranks of complete points' slots
   std::vector<uint8_t> rank_of(n_slots, 0xff);
@@ -257,10 +270,10 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
 
   // 5. per tile: tile points, descriptors, halo and constrained slots
   std::vector<TileHdr> hdr(n_tiles);
-  std::vector<uint32_t> desc(n_slots);
+  std::vector<uint32_t> desc(static_cast<std::size_t>(n_elements) * cs, 0u);
   std::vector<int32_t> htp, hslot, cslot, cidx, crow;
   std::vector<int32_t> hpos_of_slot(n_slots, -1);
-  std::vector<int32_t> tpi(ng, -1), tpi_stamp(ng, -1);
+  std::vector<int32_t> tpi(ng_dev, -1), tpi_stamp(ng, -1);
   std::vector<int32_t> block_elem_count(d.n_blocks, 0);
   for (int b = 0; b < d.n_blocks; ++b) blocks[b].e_off = 0;
   int32_t e_running = 0, hb = 0;
@@ -272,7 +285,7 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
       th.be0 = be;
       th.ne = static_cast<int32_t>(tile_elems[t].size());
       th.cbeg = cbeg[t];
-      th.nc = cbeg[t + 1] - cbeg[t];
+      th.nc = count[t + 1];  // owned points; [cbeg + nc, cbeg[t + 1]) is padding
       th.hl_off = static_cast<int32_t>(htp.size());
       th.hs_off = static_cast<int32_t>(hslot.size());
       th.cs_off = static_cast<int32_t>(cslot.size());
@@ -292,7 +305,8 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
       for (std::size_t q = 0; q < hp.size(); ++q) htp.push_back(hp[q]);
       th.ntp = th.nc + static_cast<int32_t>(hp.size());
       // tile point index of every point the tile touches
-      for (std::size_t q = 0; q < hp.size(); ++q) tpi[hp[q]] = th.nc + static_cast<int32_t>(q);
+      // halo tile points follow the complete points' padded range
+      for (std::size_t q = 0; q < hp.size(); ++q) tpi[hp[q]] = up4(th.nc) + static_cast<int32_t>(q);
       int32_t nh = 0;
       for (int el = 0; el < th.ne; ++el) {
         const int32_t e = tile_elems[t][el];
@@ -321,7 +335,7 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
             hpos_of_slot[s] = hb + nh++;
             hslot.push_back(ls);
           }
-          desc[(static_cast<std::size_t>(e_running) + be + el) * npe + k] = dsc;
+          desc[(static_cast<std::size_t>(e_running) + be + el) * cs + k] = dsc;
         }
       }
       th.nhs = nh;
@@ -333,8 +347,13 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
   }
   n_hbuf = hb;
   n_cslots = static_cast<int32_t>(crow.size());
-  tp_cap = 1;
-  for (const auto& th : hdr) tp_cap = std::max(tp_cap, th.ntp);
+  tp_cap = 4;
+  nc_cap = 4;
+  for (const auto& th : hdr) {
+    tp_cap = std::max(tp_cap, up4(th.nc) + th.ntp - th.nc);
+    nc_cap = std::max(nc_cap, up4(th.nc));
+  }
+  tp_cap = up4(tp_cap);  // keeps every component row of the staged u 16-byte aligned
 
   // 6. halo CSR and special records (device order of halo points)
   std::vector<int32_t> hoff{0}, hpos, hspec(n_halo, -1), soff{0}, swhich, coff{0}, cidx2, aidx;
@@ -405,69 +424,36 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
   }
   // mass in device numbering
   const auto mh = host_vec(d.mass, ng), imh = host_vec(d.inv_mass, ng);
-  host_mass.assign(ng, 0.0f);
-  std::vector<float> im(ng);
+  host_mass.assign(ng_dev, 0.0f);
+  std::vector<float> im(ng_dev, 0.0f);
   for (int32_t g = 0; g < ng; ++g) {
     host_mass[perm[g]] = mh[g];
     im[perm[g]] = imh[g];
   }
   mass.upload(host_mass);
   inv_mass.upload(im);
-  const std::size_t nf = static_cast<std::size_t>(ncomp) * ng;
+  const std::size_t nf = static_cast<std::size_t>(ncomp) * ng_dev;
   for (auto* buf : {&u0, &u1, &v, &a, &vn}) {
     buf->resize(nf);
     buf->zero();
   }
-  // element data of every block in tile order
-  const int ngl = ngll;
+  // element data of every block in tile order, padded layout
   for (int b = 0; b < d.n_blocks; ++b) {
-    const insem_cuda_block& src = d.blocks[b];
     std::vector<int32_t> order;  // block-local positions in tile order
     for (int t = blocks[b].tile0; t < blocks[b].tile0 + blocks[b].ntiles; ++t)
       for (int32_t e : tile_elems[t]) order.push_back(epos[e]);
-    const std::size_t n = order.size();
-    const int mstride = src.kind == INSEM_RECT ? 3 : src.kind == INSEM_AFFINE ? 5 : 5 * npe;
-    std::vector<float> met(n * mstride), c0(n * npe), c1, wr, hp, rr;
-    std::vector<uint8_t> ax;
-    const bool el = medium == INSEM_ELASTIC;
-    if (el) c1.resize(n * npe);
-    const bool axi = src.kind == INSEM_AXISYM;
-    if (axi) {
-      wr.resize(n * npe);
-      hp.resize(n * npe);
-      rr.resize(n * npe);
-      ax.resize(n);
-    }
-    for (std::size_t q = 0; q < n; ++q) {
-      const std::size_t o = order[q];
-      if (src.kind == INSEM_RECT || src.kind == INSEM_AFFINE) {
-        for (int k = 0; k < mstride; ++k) met[q * mstride + k] = src.metric[o * mstride + k];
-      } else {
-        for (int k = 0; k < npe; ++k)
-          for (int c = 0; c < 5; ++c) met[(q * 5 + c) * npe + k] = src.metric[(o * npe + k) * 5 + c];
-      }
-      for (int k = 0; k < npe; ++k) {
-        c0[q * npe + k] = src.coef0[o * npe + k];
-        if (el) c1[q * npe + k] = src.coef1[o * npe + k];
-        if (axi) {
-          wr[q * npe + k] = src.wr[o * npe + k];
-          hp[q * npe + k] = src.hoop[o * npe + k];
-          rr[q * npe + k] = src.r[o * npe + k];
-        }
-      }
-      if (axi) ax[q] = src.axial[o];
-    }
-    (void)ngl;
-    blocks[b].metric.upload(met);
-    blocks[b].coef0.upload(c0);
-    if (el) blocks[b].coef1.upload(c1);
-    if (axi) {
-      blocks[b].wr.upload(wr);
-      blocks[b].hoop.upload(hp);
-      blocks[b].r.upload(rr);
-      blocks[b].axial.upload(ax);
+    PackedBlock pk = pack_block(d.blocks[b], npe, medium, order);
+    blocks[b].metric.upload(pk.metric);
+    blocks[b].coef0.upload(pk.coef0);
+    if (medium == INSEM_ELASTIC) blocks[b].coef1.upload(pk.coef1);
+    if (d.blocks[b].kind == INSEM_AXISYM) {
+      blocks[b].wr.upload(pk.wr);
+      blocks[b].hoop.upload(pk.hoop);
+      blocks[b].r.upload(pk.r);
+      blocks[b].axial.upload(pk.axial);
     }
   }
+  ng = ng_dev;  // from here on the component stride of the device arrays
 }
 
 }  // namespace insem_b200

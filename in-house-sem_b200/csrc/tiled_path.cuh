@@ -24,8 +24,11 @@ class TiledDomain {
   // Builds tiles of at most `te` elements per block and the device numbering.
   void build(const insem_cuda_domain& d, int ngll, int te, const SpecialTerms& sp, const std::vector<float>& abs_coef);
 
-  int medium = 0, ncomp = 1, m = 0, ng = 0, npe = 0, n_elements = 0;
-  int n_complete = 0, n_halo = 0, n_tiles = 0, tp_cap = 0, n_hbuf = 0, n_cslots = 0;
+  // ng: component stride of the device arrays (points padded so that every
+  // tile's complete range starts on a 16-byte boundary); ng_ref: the
+  // reference's point count.  Halo points are [n_complete, n_complete + n_halo).
+  int medium = 0, ncomp = 1, m = 0, ng = 0, ng_ref = 0, npe = 0, n_elements = 0;
+  int n_complete = 0, n_halo = 0, n_tiles = 0, tp_cap = 0, nc_cap = 0, n_hbuf = 0, n_cslots = 0;
   bool weighted = false;
   std::vector<int32_t> perm;  // reference point -> device point
   struct BlockTiles {
@@ -60,7 +63,7 @@ struct TileLaunch {
   int block = 0;
   int parity = 0;
   StepScalars sc{};
-  const StepState* st = nullptr;
+  StepState* st = nullptr;
   double* epartial = nullptr;
   bool elastic = false;
   cudaStream_t stream = nullptr;
@@ -85,9 +88,8 @@ void launch_tiles_cfg(const TileLaunch& a) {
   const auto& b = d.blocks[a.block];
   if (b.ntiles == 0) return;
   auto go = [&](auto kernel, int nc) {
-    const size_t smem = (nc == 1)   ? TileSmem<NG, 1>::bytes(d.tp_cap)
-                        : (nc == 2) ? TileSmem<NG, 2>::bytes(d.tp_cap)
-                                    : TileSmem<NG, 3>::bytes(d.tp_cap);
+    const TileLayout L = TileLayout::make(NG, nc, b.kind, a.elastic, TileCfg<NG>::TE, d.tp_cap, d.nc_cap);
+    const size_t smem = L.total;
     // Opt in to this launch's dynamic shared memory (outside stream capture;
     // the first launch of every tile kernel happens in the uncaptured initial step).
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -96,9 +98,8 @@ void launch_tiles_cfg(const TileLaunch& a) {
       CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     INSEM_REQUIRE(smem <= 227 * 1024, INSEM_CUDA_ERR_UNSUPPORTED, "tile needs too much shared memory");
     TiledDev td = d.view(a.parity);
-    td.sdesc += static_cast<size_t>(b.e_off) * NG * NG;
-    kernel<<<b.ntiles, TileCfg<NG>::THREADS, smem, a.stream>>>(b.view(), td, a.sc, a.st, a.epartial, b.tile0,
-                                                                d.tp_cap);
+    td.sdesc += static_cast<size_t>(b.e_off) * point_stride<NG * NG>();
+    kernel<<<b.ntiles, TileCfg<NG>::THREADS, smem, a.stream>>>(b.view(), td, a.sc, a.st, a.epartial, b.tile0, L);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess)
       throw Error(INSEM_CUDA_ERR_CUDA, "tile kernel launch (ngll " + std::to_string(NG) + ", kind " +
