@@ -1,0 +1,119 @@
+// Batched solves: many independent solves (models, shots) of any ngll,
+// geometry kind, medium and azimuthal order advance together, one step of
+// every unfinished solve per batched step.
+//
+// A batched step is one CUDA graph of a fixed number of launches whatever
+// the number of solves:
+//   begin (step counters, buffer parities, modes; tile queues reset)
+//   constrained-slot gathers of every solve
+//   one persistent tile launch per tile class (ngll, kind, medium, order):
+//     CTAs pull (segment, tile) items from a device work queue
+//   halo points of every solve (elastic classes, then acoustic: the fluid's
+//     coupling term reads the solid's new acceleration)
+//   receivers (particle velocity, then recording) and energy of every solve
+// Each solve keeps its own device data, time step, parity and step count,
+// so its results are the ones it gets alone, bit for bit.  Solves that
+// reach their last step run it in final mode and leave the batch; the
+// segment tables are rebuilt and the graph re-captured when membership
+// changes.
+#pragma once
+
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "solver.cuh"
+
+namespace insem_b200 {
+
+struct TileClass {
+  int ngll = 0, kind = 0, m = 0, ncomp = 0;
+  bool elastic = false;
+  int tp_cap = 0, nc_cap = 0;  // largest tile of the class
+  std::vector<TileSeg> segs;
+  std::vector<int2> items;
+};
+
+// Host-side segment tables of one batch composition.
+struct BatchTables {
+  std::map<int, TileClass> tiles;  // key: ((ngll * 4 + kind) * 2 + elastic) * 2 + m
+  std::vector<HaloSeg> halo_segs[3];  // 1 component (acoustic), 2 and 3 components (elastic)
+  std::vector<int2> halo_items[3];
+  std::vector<ConsSeg> cons_segs;
+  std::vector<int2> cons_items;
+  std::vector<RecSeg> rec_segs;
+  std::vector<int2> pv_items, rec_items;
+  std::vector<EnergySeg> energy_segs;
+  std::vector<StepState*> states;
+};
+
+class Batch {
+ public:
+  explicit Batch(const insem_cuda_options* opt);
+  ~Batch();
+  Batch(const Batch&) = delete;
+  Batch& operator=(const Batch&) = delete;
+
+  // Builds a solve on the batch's device; returns its index.
+  int32_t add(const insem_cuda_problem& p);
+  // Takes ownership of an existing solve that no batch has stepped.
+  int32_t adopt(insem_cuda_solver* h);
+  // n batched steps (solves with fewer steps left stop at their end).
+  void advance(int32_t n);
+  // Steps until every solve is complete.
+  void run();
+  // Frees a solve (its index stays unused).
+  void remove(int32_t index);
+  insem_cuda_solver* member(int32_t index);
+  int32_t size() const { return static_cast<int32_t>(members.size()); }
+  int32_t active() const;
+  int32_t steps_to_next_completion() const;
+
+  insem_cuda_options opts{};
+  double last_ms = 0.0;           // device time of the last advance()
+  int32_t kernels_per_step = 0;   // kernel nodes of the step graph
+  int64_t point_updates = 0;      // sum of points x steps of the last advance()
+
+ private:
+  void rebuild();
+  void enqueue();
+
+  struct DevClass {
+    int ngll = 0, kind = 0, m = 0;
+    bool elastic = false;
+    DeviceBuffer<TileSeg> segs;
+    DeviceBuffer<int2> items;
+    int32_t n_items = 0;
+    TileLayout L{};
+    int grid = 0;
+  };
+
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int n_sms = 0;
+  std::vector<std::unique_ptr<insem_cuda_solver>> members;  // null after remove()
+  std::vector<char> prepared;
+  bool dirty = true;
+  cudaGraphExec_t graph = nullptr;
+  // device tables of the current composition
+  std::vector<DevClass> dclasses;
+  DeviceBuffer<int32_t> queues;
+  DeviceBuffer<HaloSeg> dhalo_segs[3];
+  DeviceBuffer<int2> dhalo_items[3];
+  int32_t n_halo_items[3] = {0, 0, 0};
+  DeviceBuffer<ConsSeg> dcons_segs;
+  DeviceBuffer<int2> dcons_items;
+  int32_t n_cons_items = 0;
+  DeviceBuffer<RecSeg> drec_segs;
+  DeviceBuffer<int2> dpv_items, drec_items;
+  int32_t n_pv_items = 0, n_rec_items = 0;
+  DeviceBuffer<EnergySeg> denergy;
+  int32_t n_energy = 0;
+  DeviceBuffer<StepState*> dstates;
+  int32_t n_states = 0;
+  DeviceBuffer<int32_t> derr;
+  int32_t* herr = nullptr;  // pinned
+  std::vector<int64_t> member_points;
+};
+
+}  // namespace insem_b200

@@ -169,5 +169,10 @@ __device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
 
 inline int ceil_div(long long a, long long b) { return static_cast<int>((a + b - 1) / b); }
+// Grid of a grid-stride loop over n items (at most 16 CTAs per SM of a B200).
+inline int grid_for(int64_t n, int threads = 256) {
+  const int64_t g = (n + threads - 1) / threads;
+  return static_cast<int>(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
+}
 
 }  // namespace insem_b200

@@ -20,15 +20,6 @@
 
 namespace insem_b200 {
 
-namespace {
-
-inline int grid_for(int64_t n, int threads = 256) {
-  const int64_t g = (n + threads - 1) / threads;
-  return static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(g, 148 * 16)));
-}
-
-}  // namespace
-
 void DeviceDomainData::upload(const insem_cuda_domain& d, const insem_cuda_basis& basis) {
   medium = d.medium;
   INSEM_REQUIRE(medium == INSEM_ACOUSTIC || medium == INSEM_ELASTIC, INSEM_CUDA_ERR_INVALID, "unknown medium");
@@ -585,6 +576,7 @@ void Solver::set_state(int32_t medium, const double* u_in, const double* v_in) {
 void Solver::advance(int32_t n) {
   DeviceGuard dg(device);
   INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
+  INSEM_REQUIRE(!in_batch, INSEM_CUDA_ERR_STATE, "this solve is stepped by a batch");
   if (tiled) {
     int32_t dummy = 0;
     advance_tiled(n, nullptr, nullptr, &dummy);
@@ -650,6 +642,7 @@ void Solver::ensure_graph() {
 
 // Per step: source amplitudes in (H2D), the step's graph, the record row out (D2H).
 void Solver::advance_streamed(int32_t n, const float* amp_in, double* rows_out, int32_t* n_rows) {
+  INSEM_REQUIRE(!in_batch, INSEM_CUDA_ERR_STATE, "this solve is stepped by a batch");
   DeviceGuard dg(device);
   INSEM_REQUIRE(n >= 0 && n_rows, INSEM_CUDA_ERR_INVALID, "invalid streamed advance");
   INSEM_REQUIRE(n_sources == 0 || amp_in, INSEM_CUDA_ERR_INVALID, "missing source amplitudes");
@@ -1005,10 +998,6 @@ void Solver::advance_tiled(int32_t n, const float* amp_in, double* rows_out, int
 }  // namespace insem_b200
 
 using namespace insem_b200;
-
-struct insem_cuda_solver {
-  std::unique_ptr<Solver> s;
-};
 
 extern "C" {
 

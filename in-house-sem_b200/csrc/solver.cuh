@@ -1,6 +1,7 @@
 // Device-resident solver state (the twin of solver::Solver).
 #pragma once
 
+#include <memory>
 #include <random>
 #include <vector>
 
@@ -38,6 +39,8 @@ struct TraceInfo {
   int32_t first_col = 0;
   int32_t ncomp = 0;
 };
+
+struct BatchTables;
 
 class Solver {
  public:
@@ -135,6 +138,25 @@ class Solver {
   bool complete = false;  // u, v, a hold step `step` (after an init or final step)
   int cur_mode = -1;
   int32_t* mode_host = nullptr;  // pinned {normal, final, init}
+
+  // ------------------------------------------------------ batched stepping
+ public:
+  bool in_batch = false;  // stepped by a Batch; advance() refuses
+  int32_t remaining() const { return n_steps - step; }
+  // Runs the initial step (if not yet run) and the predictor, leaving the
+  // fields ready for a normal step; primes the StepState's parity and last step.
+  void batch_prepare();
+  // Appends this solve's segments and work items.
+  void batch_collect(BatchTables& t);
+  // Host bookkeeping after k batched steps.
+  void batch_advanced(int32_t k);
+  // NaN/Inf check of the current fields (throws INSEM_CUDA_ERR_NONFINITE).
+  void check_fields();
 };
 
 }  // namespace insem_b200
+
+// Opaque handle of the C ABI.
+struct insem_cuda_solver {
+  std::unique_ptr<insem_b200::Solver> s;
+};

@@ -20,6 +20,8 @@ struct StepState {
   int32_t nonfinite;      // set when a NaN/Inf was found
   int32_t mode;           // tiled path: 0 normal, 1 final (state complete), 2 initial
   int32_t error;          // a bounded device-side wait gave up
+  int32_t parity;         // batched steps: field buffer parity of the current step
+  int32_t last_step;      // batched steps: the step that runs in final mode
   double kin_c;           // dt^2 / 8 of the kinetic energy (solver.cpp:903)
 };
 
@@ -210,9 +212,9 @@ __device__ __forceinline__ double interp(const ReceiversDev& r, int32_t rec, con
 
 // Particle velocity of acoustic receivers: trapezoid of -grad(p)/rho.  With
 // init != 0 only prev_a is set (Solver::initialize, solver.cpp:883-893).
-static __global__ void particle_velocity_kernel(ReceiversDev r, AllFields fl, const int32_t* __restrict__ acoustic_recv,
-                                         int32_t n_acoustic, double dt, int init) {
-  const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void particle_velocity_body(const ReceiversDev& r, const AllFields& fl,
+                                                       const int32_t* __restrict__ acoustic_recv, int32_t n_acoustic,
+                                                       double dt, int init, int32_t t) {
   if (t >= n_acoustic) return;
   const int32_t rec = acoustic_recv[t];
   const DomainFields& d = fl.d[r.domain[rec]];
@@ -233,11 +235,15 @@ static __global__ void particle_velocity_kernel(ReceiversDev r, AllFields fl, co
   pv[1] = az;
 }
 
-static __global__ void record_kernel(ReceiversDev r, AllFields fl, const RecordColumn* __restrict__ cols, int32_t n_cols,
-                              const StepState* st, int32_t record_every, double* __restrict__ traces,
-                              int32_t max_samples) {
-  const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int32_t step = st->step;
+static __global__ void particle_velocity_kernel(ReceiversDev r, AllFields fl, const int32_t* __restrict__ acoustic_recv,
+                                         int32_t n_acoustic, double dt, int init) {
+  particle_velocity_body(r, fl, acoustic_recv, n_acoustic, dt, init, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+__device__ __forceinline__ void record_body(const ReceiversDev& r, const AllFields& fl,
+                                            const RecordColumn* __restrict__ cols, int32_t n_cols, int32_t step,
+                                            int32_t record_every, double* __restrict__ traces, int32_t max_samples,
+                                            int32_t t) {
   if (t >= n_cols || step % record_every != 0) return;
   const int32_t sample = step / record_every;
   if (sample >= max_samples) return;
@@ -256,6 +262,12 @@ static __global__ void record_kernel(ReceiversDev r, AllFields fl, const RecordC
     }
   }
   traces[static_cast<size_t>(sample) * n_cols + t] = out;
+}
+
+static __global__ void record_kernel(ReceiversDev r, AllFields fl, const RecordColumn* __restrict__ cols, int32_t n_cols,
+                              const StepState* st, int32_t record_every, double* __restrict__ traces,
+                              int32_t max_samples) {
+  record_body(r, fl, cols, n_cols, st->step, record_every, traces, max_samples, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // ---------------------------------------------------------------- energy

@@ -213,9 +213,9 @@ __device__ __forceinline__ void complete_point(int mode, const StepScalars& sc, 
 }
 
 // Gathers the values of constrained slots (DofMap::gather rows, dof_map.hpp:110-115).
-static __global__ void constrained_gather_kernel(int32_t n, const int32_t* __restrict__ row_of, RowsDev rows,
-                                          const float* __restrict__ u, int32_t ng, int32_t ncomp, float* __restrict__ cval) {
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void constrained_gather_body(int32_t n, const int32_t* __restrict__ row_of, const RowsDev& rows,
+                                                        const float* __restrict__ u, int32_t ng, int32_t ncomp,
+                                                        float* __restrict__ cval, int32_t i) {
   if (i >= n) return;
   const int32_t r = row_of[i];
   for (int c = 0; c < ncomp; ++c) {
@@ -224,6 +224,12 @@ static __global__ void constrained_gather_kernel(int32_t n, const int32_t* __res
       s = fadd(s, fmul(rows.weights[q], u[static_cast<size_t>(c) * ng + rows.dofs[q]]));
     cval[static_cast<size_t>(c) * n + i] = s;
   }
+}
+
+static __global__ void constrained_gather_kernel(int32_t n, const int32_t* __restrict__ row_of, RowsDev rows,
+                                                 const float* __restrict__ u, int32_t ng, int32_t ncomp,
+                                                 float* __restrict__ cval) {
+  constrained_gather_body(n, row_of, rows, u, ng, ncomp, cval, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // Predictor on the whole field, in place (start of an advance() after a final step).
@@ -237,10 +243,15 @@ static __global__ void predictor_inplace_kernel(float* __restrict__ u, float* __
   }
 }
 
+// One tile of the fused step (the whole CTA).  `bar` is an initialised
+// mbarrier whose next phase to complete has parity `phase`.  Returns false
+// (after recording the error) if the tile's bulk copies did not arrive
+// within the wait limit.
 template <int NG, int KIND, bool EL, int M>
-static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
-    tile_step_kernel(BlockDev blk, TiledDev td, StepScalars sc, StepState* __restrict__ st,
-                     double* __restrict__ epartial, int32_t tile0, TileLayout L) {
+__device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledDev& td, const StepScalars& sc,
+                                               StepState* __restrict__ st, double* __restrict__ epartial,
+                                               int32_t tile, const TileLayout& L, unsigned char* smem_raw,
+                                               uint64_t* bar, uint32_t phase) {
   using Cfg = TileCfg<NG>;
   using CE = ElemCfg<NG, KIND, EL, M>;
   constexpr int NC = CE::NC;
@@ -249,8 +260,6 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   constexpr int ROW = Cfg::ROW;
   constexpr bool AXI = KIND == INSEM_AXISYM;
   constexpr int MS = KIND == INSEM_RECT ? 4 : KIND == INSEM_AFFINE ? 8 : 5 * CS;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + L.bar);
   float* s_metric = reinterpret_cast<float*>(smem_raw + L.metric);
   float* s_coef0 = reinterpret_cast<float*>(smem_raw + L.coef0);
   float* s_coef1 = reinterpret_cast<float*>(smem_raw + L.coef1);
@@ -267,7 +276,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   float* sax = reinterpret_cast<float*>(smem_raw + L.ax);  // [TE][4][16] axis terms
   const int tp_cap = L.tp_cap, nc_cap = L.nc_cap;
 
-  const TileHdr th = td.tiles[tile0 + blockIdx.x];
+  const TileHdr th = td.tiles[tile];
   const int tid = threadIdx.x;
   const int mode = st->mode;
   const int32_t step = st->step;
@@ -275,8 +284,6 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   const int nc4 = (th.nc + 3) & ~3;
 
   // 1. bulk copies of the tile's element data, slot descriptors and complete points
-  if (tid == 0) mbar_init(bar, 1);
-  __syncthreads();
   if (tid == 0) {
     const uint32_t eb = 4u * th.ne;
     uint32_t total = eb * MS + eb * CS * (1 + (EL ? 1 : 0) + (AXI ? 3 : 0)) + eb * CS;
@@ -306,10 +313,12 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
 #pragma unroll
     for (int c = 0; c < NC; ++c) tu[c * tp_cap + nc4 + t] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
   }
-  const bool arrived = mbar_wait_bounded(bar, 0, kBulkWaitLimit);
+  const bool arrived = mbar_wait_bounded(bar, phase, kBulkWaitLimit);
   if (__syncthreads_or(!arrived)) {
     if (tid == 0) atomicExch(&st->error, 1);
-    return;
+    // give copies still in flight a second bounded wait before the shared memory is left
+    mbar_wait_bounded(bar, phase, kBulkWaitLimit);
+    return false;
   }
 
   // element data now in shared memory, indexed by the tile-local element
@@ -510,9 +519,80 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
         k2 = dadd(k2, wk[q]);
         p2 = dadd(p2, wp[q]);
       }
-      epartial[2 * (tile0 + blockIdx.x)] = k2;
-      epartial[2 * (tile0 + blockIdx.x) + 1] = p2;
+      epartial[2 * tile] = k2;
+      epartial[2 * tile + 1] = p2;
     }
+  }
+  return true;
+}
+
+template <int NG, int KIND, bool EL, int M>
+static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
+    tile_step_kernel(BlockDev blk, TiledDev td, StepScalars sc, StepState* __restrict__ st,
+                     double* __restrict__ epartial, int32_t tile0, TileLayout L) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + L.bar);
+  if (threadIdx.x == 0) mbar_init(bar, 1);
+  __syncthreads();
+  tile_step_body<NG, KIND, EL, M>(blk, td, sc, st, epartial, tile0 + blockIdx.x, L, smem_raw, bar, 0u);
+}
+
+// Tiles of many solves in one launch.  A segment is one block of one
+// domain of one solve; its field buffers are chosen by that solve's parity.
+struct TileSeg {
+  BlockDev blk;
+  TiledDev td;          // parity-0 view (u_cur = u0, u_nxt = u1)
+  StepScalars sc;
+  StepState* st;
+  double* epartial;     // the domain's tile partials
+  int32_t tile0;        // the block's first tile in the domain's tile table
+};
+
+// Persistent CTAs take work items (segment, tile within the block) from a
+// device queue: `queue` is zeroed by the step's first kernel.  One shared
+// memory layout serves the class (sized for its largest tile).
+template <int NG, int KIND, bool EL, int M>
+static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
+    tile_batch_kernel(const TileSeg* __restrict__ segs, const int2* __restrict__ items, int32_t n_items,
+                      int32_t* __restrict__ queue, TileLayout L) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(16) TileSeg s_seg;  // the item's segment, read by the body from shared memory
+  __shared__ int32_t s_item, s_segi, s_tile;
+  static_assert(sizeof(TileSeg) % 4 == 0, "TileSeg is copied as 32-bit words");
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  uint32_t phase = 0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int32_t w = atomicAdd(queue, 1);
+      s_item = w;
+      if (w < n_items) {
+        const int2 it = items[w];
+        s_segi = it.x;
+        s_tile = it.y;
+      }
+    }
+    __syncthreads();
+    if (s_item >= n_items) break;
+    {
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(segs + s_segi);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&s_seg);
+      for (int q = threadIdx.x; q < static_cast<int>(sizeof(TileSeg) / 4); q += blockDim.x) dst[q] = src[q];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_seg.st->parity) {
+      const float* cur = s_seg.td.u_cur;
+      s_seg.td.u_cur = s_seg.td.u_nxt;
+      s_seg.td.u_nxt = const_cast<float*>(cur);
+    }
+    __syncthreads();
+    const int32_t local = s_tile;
+    const bool ok = tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial,
+                                                    s_seg.tile0 + local, L, smem_raw, &bar, phase);
+    if (!ok) break;
+    phase ^= 1u;
+    __syncthreads();  // the next item's copies overwrite shared memory
   }
 }
 
@@ -547,12 +627,13 @@ struct CouplingDev {
 // implicit Stacey solve, Dirichlet / axis zeros, and the mode's update.
 // `other` is the fluid's current pressure (solid domain) or the solid's new
 // acceleration (fluid domain), in that domain's device numbering.
+// One halo point per thread; CTAs of 256 threads, `part` = the CTA's energy partial.
 template <int NC, bool ELASTIC>
-static __global__ void __launch_bounds__(256)
-    halo_step_kernel(TiledDev td, HaloDev hd, CouplingDev cp, const float* __restrict__ other, int32_t other_ng,
-                     bool pm, const float* __restrict__ amp, int32_t n_amp, StepScalars sc, double h_damp,
-                     const StepState* __restrict__ st, double* __restrict__ epartial, int32_t epart0) {
-  const int32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev& hd, const CouplingDev& cp,
+                                               const float* __restrict__ other, int32_t other_ng, bool pm,
+                                               const float* __restrict__ amp, int32_t n_amp, const StepScalars& sc,
+                                               double h_damp, const StepState* __restrict__ st,
+                                               double* __restrict__ epartial, int32_t part, int32_t h) {
   const int mode = st->mode;
   const int32_t step = st->step;
   const bool energy = (mode == kModeInit) ? (sc.energy_every > 0) : (sc.energy_every > 0 && step % sc.energy_every == 0);
@@ -660,19 +741,28 @@ static __global__ void __launch_bounds__(256)
         k2 = dadd(k2, wk[q]);
         p2 = dadd(p2, wp[q]);
       }
-      epartial[2 * (epart0 + blockIdx.x)] = k2;
-      epartial[2 * (epart0 + blockIdx.x) + 1] = p2;
+      epartial[2 * part] = k2;
+      epartial[2 * part + 1] = p2;
     }
   }
+}
+
+template <int NC, bool ELASTIC>
+static __global__ void __launch_bounds__(256)
+    halo_step_kernel(TiledDev td, HaloDev hd, CouplingDev cp, const float* __restrict__ other, int32_t other_ng,
+                     bool pm, const float* __restrict__ amp, int32_t n_amp, StepScalars sc, double h_damp,
+                     const StepState* __restrict__ st, double* __restrict__ epartial, int32_t epart0) {
+  halo_step_body<NC, ELASTIC>(td, hd, cp, other, other_ng, pm, amp, n_amp, sc, h_damp, st, epartial,
+                              epart0 + blockIdx.x, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 // energy[sample] = (time, kinetic, potential) from the per-CTA partials of
 // the tiled step: kinetic sums all sets, potential = -0.5 x each domain's
 // u . f_int, elastic first (solver.cpp:673-678).  Partials of set d are
 // [start_d, start_d + count_d).
-static __global__ void tiled_energy_kernel(const double* __restrict__ epartial, int n_dom, int4 sets0, int4 sets1,
-                                    const StepState* __restrict__ st, int32_t energy_every, double dt,
-                                    double* __restrict__ energy, int32_t max_samples) {
+__device__ __forceinline__ void tiled_energy_body(const double* __restrict__ epartial, int n_dom, int4 sets0, int4 sets1,
+                                                  const StepState* __restrict__ st, int32_t energy_every, double dt,
+                                                  double* __restrict__ energy, int32_t max_samples) {
   __shared__ double sh[kReduceThreads];
   const int mode = st->mode;
   const int32_t step = st->step;
@@ -708,6 +798,133 @@ static __global__ void tiled_energy_kernel(const double* __restrict__ epartial, 
       energy[sample * 3 + 1] = kin;
       energy[sample * 3 + 2] = pot;
     }
+  }
+}
+
+static __global__ void tiled_energy_kernel(const double* __restrict__ epartial, int n_dom, int4 sets0, int4 sets1,
+                                           const StepState* __restrict__ st, int32_t energy_every, double dt,
+                                           double* __restrict__ energy, int32_t max_samples) {
+  tiled_energy_body(epartial, n_dom, sets0, sets1, st, energy_every, dt, energy, max_samples);
+}
+
+// ------------------------------------------------------- batched step kernels
+// The point-wise kernels of many solves in one launch each: one CTA per work
+// item (segment, chunk); the segment carries one solve's pointers and
+// scalars, the solve's StepState its step, mode and buffer parity.
+constexpr int kHaloChunk = 256;
+constexpr int kConsChunk = 128;
+constexpr int kRecChunk = 64;
+
+struct HaloSeg {
+  TiledDev td;          // parity-0 view
+  HaloDev hd;
+  CouplingDev cp;
+  const float* other0;  // coupling input at parity 0 / 1 (fluid u, or the solid's a at both)
+  const float* other1;
+  int32_t other_ng;
+  int32_t pm;
+  const float* amp;
+  int32_t n_amp;
+  StepScalars sc;
+  double h_damp;
+  const StepState* st;
+  double* epartial;
+  int32_t epart0;
+};
+
+template <int NC, bool ELASTIC>
+static __global__ void __launch_bounds__(kHaloChunk) halo_batch_kernel(const HaloSeg* __restrict__ segs,
+                                                                         const int2* __restrict__ items) {
+  const int2 it = items[blockIdx.x];
+  const HaloSeg& sg = segs[it.x];
+  const int par = sg.st->parity;
+  TiledDev td = sg.td;
+  if (par) {
+    const float* cur = td.u_cur;
+    td.u_cur = td.u_nxt;
+    td.u_nxt = const_cast<float*>(cur);
+  }
+  halo_step_body<NC, ELASTIC>(td, sg.hd, sg.cp, par ? sg.other1 : sg.other0, sg.other_ng, sg.pm != 0, sg.amp,
+                              sg.n_amp, sg.sc, sg.h_damp, sg.st, sg.epartial, sg.epart0 + it.y,
+                              it.y * kHaloChunk + static_cast<int32_t>(threadIdx.x));
+}
+
+struct ConsSeg {
+  int32_t n;
+  const int32_t* row_of;
+  RowsDev rows;
+  const float* u0;
+  const float* u1;
+  int32_t ng, ncomp;
+  float* cval;
+  const StepState* st;
+};
+
+static __global__ void __launch_bounds__(kConsChunk) constrained_batch_kernel(const ConsSeg* __restrict__ segs,
+                                                                               const int2* __restrict__ items) {
+  const int2 it = items[blockIdx.x];
+  const ConsSeg& sg = segs[it.x];
+  constrained_gather_body(sg.n, sg.row_of, sg.rows, sg.st->parity ? sg.u1 : sg.u0, sg.ng, sg.ncomp, sg.cval,
+                          it.y * kConsChunk + static_cast<int32_t>(threadIdx.x));
+}
+
+struct RecSeg {
+  ReceiversDev rv;
+  AllFields f0, f1;     // fields at parity 0 / 1
+  const int32_t* acoustic_recv;
+  int32_t n_acoustic;
+  double dt;
+  const RecordColumn* cols;
+  int32_t n_cols;
+  const StepState* st;
+  int32_t record_every;
+  double* traces;
+  int32_t max_samples;
+};
+
+static __global__ void __launch_bounds__(kRecChunk) particle_velocity_batch_kernel(const RecSeg* __restrict__ segs,
+                                                                                   const int2* __restrict__ items) {
+  const int2 it = items[blockIdx.x];
+  const RecSeg& sg = segs[it.x];
+  particle_velocity_body(sg.rv, sg.st->parity ? sg.f1 : sg.f0, sg.acoustic_recv, sg.n_acoustic, sg.dt, 0,
+                         it.y * kRecChunk + static_cast<int32_t>(threadIdx.x));
+}
+
+static __global__ void __launch_bounds__(kRecChunk) record_batch_kernel(const RecSeg* __restrict__ segs,
+                                                                        const int2* __restrict__ items) {
+  const int2 it = items[blockIdx.x];
+  const RecSeg& sg = segs[it.x];
+  record_body(sg.rv, sg.st->parity ? sg.f1 : sg.f0, sg.cols, sg.n_cols, sg.st->step, sg.record_every, sg.traces,
+              sg.max_samples, it.y * kRecChunk + static_cast<int32_t>(threadIdx.x));
+}
+
+struct EnergySeg {
+  const double* epartial;
+  int32_t n_dom;
+  int4 s0, s1;
+  const StepState* st;
+  int32_t energy_every;
+  double dt;
+  double* energy;
+  int32_t max_samples;
+};
+
+static __global__ void __launch_bounds__(kReduceThreads) energy_batch_kernel(const EnergySeg* __restrict__ segs) {
+  const EnergySeg& sg = segs[blockIdx.x];
+  tiled_energy_body(sg.epartial, sg.n_dom, sg.s0, sg.s1, sg.st, sg.energy_every, sg.dt, sg.energy, sg.max_samples);
+}
+
+// First kernel of a batched step: every solve's step counter, buffer parity
+// and mode (final on its last step), and the tile queues reset.
+static __global__ void batch_begin_kernel(StepState* const* __restrict__ sts, int32_t n, int32_t* __restrict__ queues,
+                                          int32_t n_queues) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_queues) queues[i] = 0;
+  if (i < n) {
+    StepState* s = sts[i];
+    s->step += 1;
+    s->parity ^= 1;
+    s->mode = s->step == s->last_step ? kModeFinal : kModeNormal;
   }
 }
 

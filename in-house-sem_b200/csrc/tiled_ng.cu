@@ -28,4 +28,8 @@ void INSEM_CAT(set_constant_basis_ng, INSEM_NG)(const float* D, const float* Dj,
 
 int INSEM_CAT(tile_elements_ng, INSEM_NG)() { return TileCfg<INSEM_NG>::TE; }
 
+int INSEM_CAT(tile_batch_ng, INSEM_NG)(const TileBatchLaunch& a, bool launch) {
+  return tile_batch_cfg<INSEM_NG>(a, launch);
+}
+
 }  // namespace insem_b200

@@ -83,6 +83,21 @@ void launch_tiles(int ngll, const TileLaunch& a) {
   }
 }
 
+int tile_batch(int ngll, const TileBatchLaunch& a, bool launch) {
+  switch (ngll) {
+    case 2: return tile_batch_ng2(a, launch);
+    case 3: return tile_batch_ng3(a, launch);
+    case 4: return tile_batch_ng4(a, launch);
+    case 5: return tile_batch_ng5(a, launch);
+    case 6: return tile_batch_ng6(a, launch);
+    case 7: return tile_batch_ng7(a, launch);
+    case 8: return tile_batch_ng8(a, launch);
+    case 9: return tile_batch_ng9(a, launch);
+    default: check_ngll(ngll);
+  }
+  return 0;
+}
+
 BlockDev TiledDomain::BlockTiles::view() const {
   BlockDev v;
   v.kind = kind;

@@ -82,6 +82,67 @@ int tile_elements(int ngll);  // TileCfg<NG>::TE
 void set_constant_basis(int ngll, const std::vector<float>& D, const std::vector<float>& Dj,
                         const std::vector<float>& w2);
 
+// Batched tile launches: one persistent launch per tile class (ngll, kind,
+// medium, order) over the work items of many solves.
+struct TileBatchLaunch {
+  int kind = 0, m = 0;
+  bool elastic = false;
+  const TileSeg* segs = nullptr;
+  const int2* items = nullptr;
+  int32_t n_items = 0;
+  int32_t* queue = nullptr;
+  TileLayout L{};  // the class layout; its total is the dynamic shared memory
+  uint32_t smem = 0;
+  int grid = 0;
+  cudaStream_t stream = nullptr;
+};
+// launch == false: sets the class kernel's dynamic shared memory (outside
+// stream capture) and returns its resident CTAs per SM; true: launches.
+int tile_batch_ng2(const TileBatchLaunch&, bool launch);
+int tile_batch_ng3(const TileBatchLaunch&, bool launch);
+int tile_batch_ng4(const TileBatchLaunch&, bool launch);
+int tile_batch_ng5(const TileBatchLaunch&, bool launch);
+int tile_batch_ng6(const TileBatchLaunch&, bool launch);
+int tile_batch_ng7(const TileBatchLaunch&, bool launch);
+int tile_batch_ng8(const TileBatchLaunch&, bool launch);
+int tile_batch_ng9(const TileBatchLaunch&, bool launch);
+int tile_batch(int ngll, const TileBatchLaunch& a, bool launch);
+
+template <int NG>
+int tile_batch_cfg(const TileBatchLaunch& a, bool launch) {
+  INSEM_REQUIRE(a.smem <= 227u * 1024u, INSEM_CUDA_ERR_UNSUPPORTED, "tile needs too much shared memory");
+  auto go = [&](auto kernel) -> int {
+    if (!launch) {
+      CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(a.smem)));
+      int nb = 0;
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, TileCfg<NG>::THREADS, a.smem));
+      return nb;
+    }
+    kernel<<<a.grid, TileCfg<NG>::THREADS, a.smem, a.stream>>>(a.segs, a.items, a.n_items, a.queue, a.L);
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess)
+      throw Error(INSEM_CUDA_ERR_CUDA, "batched tile kernel launch (ngll " + std::to_string(NG) + ", kind " +
+                                           std::to_string(a.kind) + ", grid " + std::to_string(a.grid) + ", smem " +
+                                           std::to_string(a.smem) + "): " + cudaGetErrorString(err));
+    return 0;
+  };
+  if (a.kind == INSEM_AXISYM) {
+    if (a.m == 1) return a.elastic ? go(tile_batch_kernel<NG, INSEM_AXISYM, true, 1>)
+                                   : go(tile_batch_kernel<NG, INSEM_AXISYM, false, 1>);
+    return a.elastic ? go(tile_batch_kernel<NG, INSEM_AXISYM, true, 0>) : go(tile_batch_kernel<NG, INSEM_AXISYM, false, 0>);
+  }
+  switch (a.kind) {
+    case INSEM_RECT:
+      return a.elastic ? go(tile_batch_kernel<NG, INSEM_RECT, true, 0>) : go(tile_batch_kernel<NG, INSEM_RECT, false, 0>);
+    case INSEM_AFFINE:
+      return a.elastic ? go(tile_batch_kernel<NG, INSEM_AFFINE, true, 0>)
+                       : go(tile_batch_kernel<NG, INSEM_AFFINE, false, 0>);
+    default:
+      return a.elastic ? go(tile_batch_kernel<NG, INSEM_CURVED, true, 0>)
+                       : go(tile_batch_kernel<NG, INSEM_CURVED, false, 0>);
+  }
+}
+
 template <int NG>
 void launch_tiles_cfg(const TileLaunch& a) {
   const TiledDomain& d = *a.dom;

@@ -138,6 +138,20 @@ def lib() -> C.CDLL:
             "insem_cuda_solver_advance_streamed": (C.c_int, [vp, C.c_int32, f32p, f64p, i32p]),
             "insem_cuda_solver_n_columns": (C.c_int32, [vp]),
             "insem_cuda_solver_kernels_per_step": (C.c_int32, [vp]),
+            "insem_cuda_batch_create": (C.c_int, [C.POINTER(Options), C.POINTER(vp)]),
+            "insem_cuda_batch_destroy": (None, [vp]),
+            "insem_cuda_batch_add": (C.c_int, [vp, C.POINTER(Problem), i32p]),
+            "insem_cuda_batch_adopt": (C.c_int, [vp, vp, i32p]),
+            "insem_cuda_batch_advance": (C.c_int, [vp, C.c_int32]),
+            "insem_cuda_batch_run": (C.c_int, [vp]),
+            "insem_cuda_batch_remove": (C.c_int, [vp, C.c_int32]),
+            "insem_cuda_batch_member": (vp, [vp, C.c_int32]),
+            "insem_cuda_batch_size": (C.c_int32, [vp]),
+            "insem_cuda_batch_active": (C.c_int32, [vp]),
+            "insem_cuda_batch_steps_to_next_completion": (C.c_int32, [vp]),
+            "insem_cuda_batch_last_advance_ms": (C.c_double, [vp]),
+            "insem_cuda_batch_point_updates": (C.c_int64, [vp]),
+            "insem_cuda_batch_kernels_per_step": (C.c_int32, [vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)

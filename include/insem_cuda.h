@@ -291,6 +291,42 @@ int32_t insem_cuda_solver_kernels_per_step(insem_cuda_solver* h);
  * iteration counts, FP64 reductions on the device; returns 2/sqrt(lambda). */
 int insem_cuda_stable_dt(const insem_cuda_problem* problem, int32_t device, double* stable_dt);
 
+/* ---------------------------------------------------------- batched solves */
+/* Many independent solves (models, shots) of any ngll, geometry kind, medium
+ * and azimuthal order, advanced together: every batched step is one CUDA
+ * graph of a fixed number of launches (persistent tile launches per tile
+ * class fed by a device work queue, then the point-wise kernels of all
+ * solves).  Each solve keeps its own time step and step count and gets the
+ * results it gets alone, bit for bit.  The reference has no batch API; its
+ * nearest form is one Simulation per thread (bindings.cpp:336-337).
+ * Members are insem_cuda_solver handles owned by the batch: read them with
+ * the insem_cuda_solver_* accessors (set_state before the first batched
+ * step), never destroy them and never advance them directly. */
+typedef struct insem_cuda_batch insem_cuda_batch;
+int insem_cuda_batch_create(const insem_cuda_options* options, insem_cuda_batch** out);
+void insem_cuda_batch_destroy(insem_cuda_batch* h);
+/* Builds a solve (device upload) and appends it; *index (may be NULL) is its index. */
+int insem_cuda_batch_add(insem_cuda_batch* h, const insem_cuda_problem* problem, int32_t* index);
+/* Takes ownership of a solver handle that has not been stepped by a batch. */
+int insem_cuda_batch_adopt(insem_cuda_batch* h, insem_cuda_solver* solver, int32_t* index);
+/* n batched steps; a solve with fewer steps left stops at its last step. */
+int insem_cuda_batch_advance(insem_cuda_batch* h, int32_t n);
+/* Steps until every member is complete. */
+int insem_cuda_batch_run(insem_cuda_batch* h);
+/* Frees a member (indices of the others are unchanged). */
+int insem_cuda_batch_remove(insem_cuda_batch* h, int32_t index);
+/* Borrowed handle of member `index` (NULL and an error message if there is none). */
+insem_cuda_solver* insem_cuda_batch_member(insem_cuda_batch* h, int32_t index);
+int32_t insem_cuda_batch_size(const insem_cuda_batch* h);
+int32_t insem_cuda_batch_active(const insem_cuda_batch* h);
+/* Steps until the next member completes (0 when none is running). */
+int32_t insem_cuda_batch_steps_to_next_completion(const insem_cuda_batch* h);
+/* Device time of the last advance / run segment, ms; points x steps it did. */
+double insem_cuda_batch_last_advance_ms(const insem_cuda_batch* h);
+int64_t insem_cuda_batch_point_updates(const insem_cuda_batch* h);
+/* Kernel nodes of the current batched-step graph. */
+int32_t insem_cuda_batch_kernels_per_step(const insem_cuda_batch* h);
+
 #ifdef __cplusplus
 }
 #endif
