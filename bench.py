@@ -1,29 +1,37 @@
 """Benchmark of insem's per-time-step path on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--nx 1024]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload batched|config3] [--models 256] [--nx 1024]
 
-Workload (default): the large coupled Cartesian model -- 1024 x 1024 order-5
-elements over 400 m x 400 m, 60 m of water over 8 curved elastic layers,
-~26.2M unique GLL points -- built by the native setup from seeded synthetic
-parameters (there is no dataset; shapes and value ranges as the benchmark
-configuration states them).  A "step" is one central-difference time step of
-the whole model.  Metric: GLL-point-updates/s = unique global points summed
-over domains x steps / seconds.
+Metric: GLL-point-updates/s = unique global points summed over domains and
+solves x steps / seconds (setup and the stable-dt power iteration excluded).
 
-value      device time (CUDA events on the solver's stream) of K steps with
-           every input resident in HBM; the step touches ~2 GB, larger than
-           L2, so no flush is needed.
-e2e        the same metric through the C ABI's streamed advance: every step
-           copies its source amplitudes in from pinned host memory and its
-           receiver sample row (512 receivers) back, wall clock.
-roofline   HBM roofline of the whole step: algorithmic bytes per step (the
-           fixed B_step formula, ProblemData.algorithmic_bytes_per_step) over
-           the step time, against the measured copy bandwidth.
-cpu_baseline  the reference's own CPU/OpenMP time loop (oracle build) on the
-           same model at 1/16 of the elements (256 x 256), all host cores.
+Default workload (batched): 256 independent axisymmetric borehole models
+(seeded: hole radius, monopole / dipole half each, 1-6 beds incl. slow
+formations, casing in 30 %, GLL order 4-6, 5k-80k elements after AMR, 13
+receivers, 5 ms), built by the native setup.  A step is one batched step:
+one time step of every model (each with its own dt).
+
+value      device time (CUDA events) of K batched steps, every input resident
+           in HBM; a batched step touches ~15 GB, far more than L2.
+plain      the same models with the plain one-solve-per-launch path (each
+           solve's own step graph, solves one after another), device time.
+e2e        the same metric through the C ABI's streamed batched steps: every
+           step copies all models' source amplitudes in from pinned host
+           memory and all models' sample rows back, wall clock.
+roofline   HBM roofline of the tile kernels (the dominant launches): their
+           algorithmic bytes per batched step (element terms + points finished
+           in tiles, the fixed B_step formula split by point class) over their
+           CUDA-event time per step, measured on plain launches after the
+           timed region; step_roofline: the whole step's B_step over the
+           timed step time.
+plain_config3  the large coupled Cartesian model (1024 x 1024 order-5
+           elements, ~26.2M points) on the plain path: value and roofline.
+cpu_baseline  the reference's own CPU/OpenMP time loop (oracle build) on a
+           sample of the same models, all host cores.
 
 With --gpus N > 1 (torchrun) every rank runs an independent replica (the
-path has no exchange step); value = N x per-replica points x steps / the
+path has no exchange step); value = sum over ranks of point-updates / the
 slowest rank's time.
 """
 
@@ -139,18 +147,22 @@ def barrier(pg, device: int):
     torch.cuda.synchronize(device)
 
 
-def cpu_baseline(warmup: int, steps: int) -> dict:
-    """The reference's CPU loop on the 1/16 sample (or the oracle port if the reference build is absent)."""
+def _cpu_env():
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    return cores
+
+
+def cpu_baseline_config3(warmup: int, steps: int) -> dict:
+    """The reference's CPU loop on config3 at 1/16 of the elements (or the oracle port without the reference build)."""
     import __graft_entry__ as entry
 
     entry.load_package()
     from insem_b200 import cases as K
 
-    cores = os.cpu_count() or 1
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    os.environ.setdefault("OMP_PROC_BIND", "close")
+    cores = _cpu_env()
     model = K.config3(nx=REF_SAMPLE_NX, n_receivers=128)
-    sys.path.insert(0, str(REPO))
     from oracle import refbench
 
     if refbench.available():
@@ -158,7 +170,7 @@ def cpu_baseline(warmup: int, steps: int) -> dict:
         return {"value": r["points"] * steps / r["seconds"], "unit": METRIC, "cores": cores, "kind": "reference",
                 "sample": f"config3 at nx={REF_SAMPLE_NX} ({r['elements']} elements, {int(r['points'])} points), "
                           f"{steps} steps after {warmup}; setup {r['setup_seconds']:.1f} s excluded",
-                "seconds": r["seconds"]}
+                "seconds": r["seconds"], "steps": steps}
     import oracle
 
     prob = K.build(model, stable_dt=None)
@@ -169,35 +181,84 @@ def cpu_baseline(warmup: int, steps: int) -> dict:
     s.advance(steps)
     sec = time.perf_counter() - t0
     return {"value": prob.n_global_total() * steps / sec, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": f"config3 at nx={REF_SAMPLE_NX}, {steps} steps (oracle port, 1 thread)", "seconds": sec}
+            "sample": f"config3 at nx={REF_SAMPLE_NX}, {steps} steps (oracle port, 1 thread)", "seconds": sec,
+            "steps": steps}
+
+
+def cpu_baseline_config4(warmup: int, steps: int, sample_models: int = 4) -> dict:
+    """The reference's CPU loop on the first `sample_models` batched borehole
+    models in sequence, each on all host cores, at the dt the device uses
+    (or the oracle port without the reference build)."""
+    import __graft_entry__ as entry
+
+    entry.load_package()
+    from insem_b200 import cases as K
+
+    cores = _cpu_env()
+    from oracle import refbench
+
+    params = K.config4_params(256, 4)[:sample_models]
+    geo = K.config4_geometry_table(256, 4)
+    updates, seconds, elems = 0.0, 0.0, 0
+    if refbench.available():
+        for i, p in enumerate(params):
+            model = K.config4_model(p, *(geo[i] if geo else (6.0, 4.0)))
+            r = refbench.run(model, 0.0, warmup, steps)
+            updates += r["points"] * steps
+            seconds += r["seconds"]
+            elems += r["elements"]
+        return {"value": updates / seconds, "unit": METRIC, "cores": cores, "kind": "reference",
+                "sample": f"config4 models 0-{sample_models - 1} ({elems} elements) in sequence, {steps} steps each "
+                          f"after {warmup}, reference dt; setup excluded",
+                "seconds": seconds, "steps": steps}
+    import oracle
+
+    for i, p in enumerate(params):
+        model = K.config4_model(p, *(geo[i] if geo else (6.0, 4.0)))
+        prob = K.build(model, stable_dt=1e-7)
+        prob.n_steps = warmup + steps
+        s = oracle.OracleSolver(prob)
+        s.advance(warmup)
+        t0 = time.perf_counter()
+        s.advance(steps)
+        seconds += time.perf_counter() - t0
+        updates += prob.n_global_total() * steps
+    return {"value": updates / seconds, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"config4 models 0-{sample_models - 1}, {steps} steps each (oracle port, 1 thread)",
+            "seconds": seconds, "steps": steps}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    base = cpu_baseline(args.warmup, args.steps)
+    if args.workload == "config3":
+        base = cpu_baseline_config3(args.warmup, args.cpu_steps)
+        workload = f"config3 coupled 2D Cartesian, order 5, sample nx={REF_SAMPLE_NX}"
+    else:
+        base = cpu_baseline_config4(max(1, min(args.warmup, 2)), args.cpu_steps)
+        workload = "config4 batched boreholes (reference: models in sequence, all host cores)"
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": METRIC, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * base["seconds"] / args.steps,
+            "steps": base["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * base["seconds"] / base["steps"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)",
-            "config": {"workload": f"config3 coupled 2D Cartesian, order 5, sample nx={REF_SAMPLE_NX}",
-                       "l2": "inputs larger than L2"},
+            "data": "synthetic (seeded model parameters)",
+            "config": {"workload": workload, "l2": "inputs larger than L2"},
             "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": base["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_ours(args, world, rank, local, pg):
+def bench_config3(args, world, rank, device, pg, headline: bool) -> dict:
+    """The large coupled Cartesian model on the plain path."""
     import torch
 
     import __graft_entry__ as entry
 
     pkg = entry.load_package()
     from insem_b200 import cases as K
+    from insem_b200.stf import amplitudes
 
-    device = local
-    torch.cuda.set_device(device)
-    total_steps = args.warmup + 2 * args.steps + 2
+    steps = args.steps if headline else args.config3_steps
+    total_steps = args.warmup + 2 * steps + 2
     model = K.config3(nx=args.nx, n_steps=total_steps)
     t0 = time.perf_counter()
     prob = K.build(model, device=device, stable_dt=args.stable_dt)
@@ -205,63 +266,180 @@ def run_ours(args, world, rank, local, pg):
     solver = pkg.Solver(prob, device=device, use_graphs=not args.no_graphs)
     solver.advance(args.warmup)
     kps = solver.kernels_per_step if not args.no_graphs else None
-
     barrier(pg, device)
     with ClockSampler(device) as clocks:
-        solver.advance(args.steps)
+        solver.advance(steps)
         barrier(pg, device)
     ms = reduce_max(pg, solver.last_advance_ms, device)
     points = prob.n_global_total()
-    value = world * points * args.steps / (ms * 1e-3)
-
-    # e2e: per-step amplitudes in from pinned memory, sample rows out, wall clock
-    from insem_b200.stf import amplitudes
-
-    if args.no_e2e:
-        if rank == 0:
-            print(json.dumps({"metric": METRIC, "value": world * prob.n_global_total() * args.steps / (ms * 1e-3),
-                              "ms_per_step": ms / args.steps, "note": "profiling run (no e2e, no baseline)"}))
-        solver.close()
-        return
-
-    s0 = solver.step
-    amp = torch.empty((args.steps, len(prob.sources)), dtype=torch.float32).pin_memory()
-    amp.numpy()[:] = amplitudes(prob, s0 + 1, args.steps)
-    rows = torch.empty((args.steps + 1, max(solver.n_columns, 1)), dtype=torch.float64).pin_memory()
-    barrier(pg, device)
-    t0 = time.perf_counter()
-    n_rows = solver.advance_streamed(args.steps, amp.numpy(), rows.numpy())
-    wall = time.perf_counter() - t0
-    wall = reduce_max(pg, wall, device)
-    e2e = world * points * args.steps / wall
-
     hbm, how = peaks()
     b_step = prob.algorithmic_bytes_per_step()
-    achieved = b_step / (ms * 1e-3 / args.steps) / 1e9
+    achieved = b_step / (ms * 1e-3 / steps) / 1e9
+    out = {"value": world * points * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
+           "workload": f"config3 coupled 2D Cartesian {args.nx}x{args.nx} order 5 (water over 8 curved elastic layers)",
+           "points": points, "elements": prob.n_elements_total(), "setup_seconds": round(setup_s, 1),
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                        "traffic": None, "kernel": "whole step (all kernels of one step)",
+                        "algorithmic_bytes_per_step": b_step, "peak_source": how},
+           "kernels_per_step": kps, "clocks": clocks.summary()}
+    if headline and not args.no_e2e:
+        s0 = solver.step
+        amp = torch.empty((steps, len(prob.sources)), dtype=torch.float32).pin_memory()
+        amp.numpy()[:] = amplitudes(prob, s0 + 1, steps)
+        rows = torch.empty((steps + 1, max(solver.n_columns, 1)), dtype=torch.float64).pin_memory()
+        barrier(pg, device)
+        t0 = time.perf_counter()
+        n_rows = solver.advance_streamed(steps, amp.numpy(), rows.numpy())
+        wall = reduce_max(pg, time.perf_counter() - t0, device)
+        out["e2e"] = {"value": world * points * steps / wall, "unit": METRIC, "h2d_bytes_per_step": 4 * len(prob.sources),
+                      "d2h_bytes_per_step": 8 * solver.n_columns, "rows": n_rows}
+    solver.close()
+    return out
+
+
+def build_config4(args, device):
+    """The batched borehole models as (params, problem, solver); setups in a thread pool."""
+    import __graft_entry__ as entry
+
+    pkg = entry.load_package()
+    from insem_b200 import cases as K
+
+    out = []
+    for p, model, arrays, ne, geo in K.config4(args.models, 4):
+        prob = K.build_from_arrays(model, arrays, device=device)
+        del arrays
+        out.append((p, prob, pkg.Solver(prob, device=device, use_graphs=not args.no_graphs)))
+    return out
+
+
+def bench_config4(args, world, rank, device, pg) -> dict:
+    import torch
+
+    import __graft_entry__ as entry
+
+    pkg = entry.load_package()
+    from insem_b200.stf import amplitudes
+
+    t0 = time.perf_counter()
+    models = build_config4(args, device)
+    setup_s = time.perf_counter() - t0
+    points = sum(prob.n_global_total() for _, prob, _ in models)
+    elements = sum(prob.n_elements_total() for _, prob, _ in models)
+    b_step = sum(prob.algorithmic_bytes_per_step() for _, prob, _ in models)
+    split = [s.algorithmic_bytes_split() for _, _, s in models]
+    tile_bytes = sum(t for t, _ in split)
+
+    # plain: every solve alone, its own step graph, one after another
+    plain_ms, plain_updates = 0.0, 0
+    for _, prob, s in models:
+        s.advance(args.warmup)
+        s.advance(args.plain_steps)
+        plain_ms += s.last_advance_ms
+        plain_updates += prob.n_global_total() * args.plain_steps
+    plain_ms = reduce_max(pg, plain_ms, device)
+    plain_value = world * plain_updates / (plain_ms * 1e-3)
+
+    # batched
+    batch = pkg.Batch(device=device, use_graphs=not args.no_graphs)
+    members = [batch.adopt(s) for _, _, s in models]
+    batch.advance(args.warmup)
+    barrier(pg, device)
+    with ClockSampler(device) as clocks:
+        batch.advance(args.steps)
+        barrier(pg, device)
+    updates = batch.point_updates
+    ms = reduce_max(pg, batch.last_advance_ms, device)
+    value = world * updates / (ms * 1e-3)
+    kps = batch.kernels_per_step if not args.no_graphs else None
+
+    line_e2e = None
+    if not args.no_e2e:
+        k = min(args.steps, batch.steps_to_next_completion)
+        act = batch.active_members()
+        amp_cols, row_cols = batch.stream_layout()
+        amp = torch.empty((k, max(amp_cols, 1)), dtype=torch.float32).pin_memory()
+        an = amp.numpy()
+        col = 0
+        for m in act:
+            nsrc = len(m.problem.sources)
+            an[:, col:col + nsrc] = amplitudes(m.problem, m.step + 1, k)
+            col += nsrc
+        rows = torch.empty((k, max(row_cols, 1)), dtype=torch.float64).pin_memory()
+        barrier(pg, device)
+        t0 = time.perf_counter()
+        done = batch.advance_streamed(k, amp, rows)
+        wall = reduce_max(pg, time.perf_counter() - t0, device)
+        line_e2e = {"value": world * batch.point_updates / wall, "unit": METRIC, "h2d_bytes_per_step": 4 * amp_cols,
+                    "d2h_bytes_per_step": 8 * row_cols, "steps": done}
+
+    # dominant launches: the tile kernels, CUDA events around them on plain launches
+    tile_ms, step_ms = batch.profile(args.profile_steps)
+    hbm, how = peaks()
+    per_step_tile_s = tile_ms * 1e-3 / args.profile_steps
+    achieved = tile_bytes / per_step_tile_s / 1e9
+    step_achieved = b_step / (ms * 1e-3 / args.steps) / 1e9
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model parameters)",
-        "config": {"workload": f"config3 coupled 2D Cartesian {args.nx}x{args.nx} order 5 (water over 8 curved "
-                               f"elastic layers)", "points": points, "elements": prob.n_elements_total(),
+        "config": {"workload": f"config4: {len(models)} axisymmetric borehole models batched (GLL order 4-6, "
+                               f"m=0/1 half each, 5k-80k elements, casing in 30 %)",
+                   "models": len(models), "points": points, "elements": elements,
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (~2 GB touched per step)", "setup_seconds": round(setup_s, 1)},
-        "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": 4 * len(prob.sources),
-                "d2h_bytes_per_step": 8 * solver.n_columns, "rows": n_rows},
+                   "l2": f"inputs larger than L2 (~{b_step / 1e9:.1f} GB touched per batched step)",
+                   "setup_seconds": round(setup_s, 1)},
+        "plain": {"value": plain_value, "unit": METRIC, "steps_per_model": args.plain_steps,
+                  "ms_total": plain_ms, "path": "one solve per launch: each model's own step graph, in sequence"},
+        "batched_over_plain": value / plain_value,
+        "e2e": line_e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": "whole step (all kernels of one step)",
-                     "algorithmic_bytes_per_step": b_step, "peak_source": how},
+                     "traffic": None, "kernel": "tile_batch_kernel (all tile classes of one batched step)",
+                     "algorithmic_bytes_per_launch_group": tile_bytes, "ms_per_launch_group": tile_ms / args.profile_steps,
+                     "tile_share_of_step": tile_ms / step_ms if step_ms > 0 else None, "peak_source": how},
+        "step_roofline": {"achieved": step_achieved, "frac": step_achieved / hbm, "algorithmic_bytes_per_step": b_step},
         "gpu_launches": (kps or 0) * args.steps,
         "kernels_per_step": kps,
         "clocks": clocks.summary(),
     }
+    batch.close()
+    return line
+
+
+def run_ours(args, world, rank, local, pg):
+    import torch
+
+    device = local
+    torch.cuda.set_device(device)
+    if args.workload == "config3":
+        r = bench_config3(args, world, rank, device, pg, headline=True)
+        line = {
+            "metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": world, "steps": r["steps"],
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded model parameters)",
+            "config": {"workload": r["workload"], "points": r["points"], "elements": r["elements"],
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (~2 GB touched per step)", "setup_seconds": r["setup_seconds"]},
+            "e2e": r.get("e2e"), "roofline": r["roofline"],
+            "gpu_launches": (r["kernels_per_step"] or 0) * r["steps"], "kernels_per_step": r["kernels_per_step"],
+            "clocks": r["clocks"],
+        }
+    else:
+        line = bench_config4(args, world, rank, device, pg)
+        if not args.no_config3:
+            r = bench_config3(args, world, rank, device, pg, headline=False)
+            line["plain_config3"] = {k: r[k] for k in ("value", "ms_per_step", "steps", "workload", "points",
+                                                        "roofline", "clocks")}
+            line["gpu_launches"] += (r["kernels_per_step"] or 0) * r["steps"]
     if rank == 0 and not args.no_cpu:
         try:
-            line["cpu_baseline"] = {k: v for k, v in cpu_baseline(1, args.cpu_steps).items() if k != "seconds"}
+            if args.workload == "config3":
+                base = cpu_baseline_config3(1, args.cpu_steps)
+            else:
+                base = cpu_baseline_config4(1, args.cpu_steps)
+            line["cpu_baseline"] = {k: v for k, v in base.items() if k not in ("seconds", "steps")}
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": METRIC, "cores": 0, "kind": "unavailable",
                                     "sample": str(exc)[:200]}
-    solver.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -269,16 +447,22 @@ def run_ours(args, world, rank, local, pg):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--workload", choices=["batched", "config3"], default="batched")
+    ap.add_argument("--models", type=int, default=256, help="batched workload: number of models")
+    ap.add_argument("--plain-steps", type=int, default=20, help="batched workload: steps per model on the plain path")
+    ap.add_argument("--profile-steps", type=int, default=5, help="steps of the event-timed tile profile")
+    ap.add_argument("--nx", type=int, default=1024, help="config3 elements per side")
+    ap.add_argument("--config3-steps", type=int, default=200, help="steps of the config3 sub-run")
+    ap.add_argument("--no-config3", action="store_true", help="skip the config3 sub-run")
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the streamed end-to-end run")
-    ap.add_argument("--no-graphs", action="store_true", help="plain launches instead of the step graph")
+    ap.add_argument("--no-graphs", action="store_true", help="plain launches instead of the step graphs")
     ap.add_argument("--stable-dt", type=float, default=None,
-                    help="use this stable time step instead of the device power iteration (profiling runs)")
+                    help="config3: use this stable time step instead of the device power iteration (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local, pg = dist_setup(args.gpus)

@@ -15,7 +15,7 @@ thread (python/src/bindings.cpp:336-337).
 from __future__ import annotations
 
 import ctypes as C
-from typing import List, Optional
+from typing import List, Optional, Tuple
 
 from . import native as N
 from .problem import ProblemData
@@ -98,6 +98,40 @@ class Batch:
 
     def run(self) -> None:
         N.check(N.lib().insem_cuda_batch_run(self._h))
+
+    def stream_layout(self):
+        """(amplitude columns, sample-row columns) of the streamed steps of the
+        current composition: active members in index order."""
+        a, r = C.c_int32(), C.c_int32()
+        N.check(N.lib().insem_cuda_batch_stream_layout(self._h, C.byref(a), C.byref(r)))
+        return a.value, r.value
+
+    def active_members(self) -> List["BatchMember"]:
+        return [m for m in self.members if m is not None and m.step < m.n_steps]
+
+    def advance_streamed(self, n_steps: int, amplitudes, rows_out=None) -> int:
+        """Up to n_steps batched steps (stopping at the next completion) with
+        per-step host I/O: ``amplitudes`` [n_steps, amp_cols] float32 in,
+        ``rows_out`` [n_steps, row_cols] float64 out (numpy arrays or pinned
+        torch tensors).  Returns the steps done."""
+        def ptr(x, ctype):
+            if x is None:
+                return None
+            if hasattr(x, "data_ptr"):
+                return C.cast(C.c_void_p(x.data_ptr()), C.POINTER(ctype))
+            return x.ctypes.data_as(C.POINTER(ctype))
+
+        done = C.c_int32()
+        N.check(N.lib().insem_cuda_batch_advance_streamed(self._h, int(n_steps), ptr(amplitudes, C.c_float),
+                                                          ptr(rows_out, C.c_double), C.byref(done)))
+        return done.value
+
+    def profile(self, n_steps: int) -> Tuple[float, float]:
+        """n steps with plain launches and CUDA events around each step's tile
+        launches: (device ms of the tile launches, device ms of the steps)."""
+        t, st = C.c_double(), C.c_double()
+        N.check(N.lib().insem_cuda_batch_profile(self._h, int(n_steps), C.byref(t), C.byref(st)))
+        return t.value, st.value
 
     @property
     def active(self) -> int:

@@ -101,7 +101,11 @@ def rectangle(x, z, nx=None, nz=None, material: Union[int, Sequence[int], Callab
     zl = np.repeat(_lattice(zs, quadratic)[:, None], xl.size, axis=1)
     if callable(material):
         xc, zc = 0.5 * (xs[:-1] + xs[1:]), 0.5 * (zs[:-1] + zs[1:])
-        mat = np.array([material(xc[i], zc[j]) for j in range(ncz) for i in range(ncx)], np.int32)
+        if getattr(material, "vectorized", False):  # takes the cell-centre arrays (row-major, x fastest)
+            X, Z = np.meshgrid(xc, zc)
+            mat = np.asarray(material(X.ravel(), Z.ravel()), np.int32)
+        else:
+            mat = np.array([material(xc[i], zc[j]) for j in range(ncz) for i in range(ncx)], np.int32)
     else:
         mat = np.broadcast_to(np.asarray(material, np.int32), (ncx * ncz,)).copy()
     return _structured(xl, zl, quadratic, mat, coords == "axisymmetric")
@@ -172,11 +176,16 @@ def borehole(z, annuli, formation_radius, beds=(), dz=0.05, dr=None, growth=1.3,
         names.setdefault(name, len(names) + 1)
     bottoms = np.array([b[0] for b in beds])
 
+    bed_ids = np.array([names[b[1]] for b in beds], np.int32)
+
     def region(rc, zc):
-        for name, outer in annuli:
-            if rc < outer:
-                return names[name]
-        return names[beds[int(np.searchsorted(bottoms, zc, side="right")) - 1][1]]
+        rc, zc = np.asarray(rc, float), np.asarray(zc, float)
+        out = bed_ids[np.searchsorted(bottoms, zc, side="right") - 1]
+        for name, outer in reversed(annuli):  # the innermost annulus containing the cell wins
+            out = np.where(rc < outer, names[name], out)
+        return out
+
+    region.vectorized = True
 
     m = rectangle(r_breaks, z_breaks, material=region, quadratic=quadratic, coords="axisymmetric")
     return Borehole(m, names, {"bottom": BOTTOM, "outer": RIGHT, "top": TOP, "axis": LEFT})
@@ -364,9 +373,15 @@ def describe(model: Model):
 
 def build(model: Model, device: int = 0, stable_dt: Optional[float] = None) -> ProblemData:
     """Native setup, then dt = safety x the device power-iteration estimate (or model.dt)."""
+    return build_from_arrays(model, setup_arrays(model), device, stable_dt)
+
+
+def build_from_arrays(model: Model, arrays: Dict[str, np.ndarray], device: int = 0,
+                      stable_dt: Optional[float] = None) -> ProblemData:
+    """``build`` on the output of ``setup_arrays`` (which may run in worker threads)."""
     from .solver import estimate_stable_dt
 
-    arrays = setup_arrays(model)
+    arrays = dict(arrays)
     arrays["problem.dt"] = np.asarray(1.0)
     arrays["problem.n_steps"] = np.asarray(0)
     arrays["problem.stable_dt"] = np.asarray(0.0)
@@ -442,3 +457,142 @@ def config3(nx: int = 1024, n_steps: int = 2000, seed: int = 3, n_receivers: int
                  boundaries={BOTTOM: "absorbing", LEFT: "absorbing", RIGHT: "absorbing", TOP: "free"},
                  sources=[Source("force", 200.0, -20.0, (0.0, 1.0, 0.0), ricker(30.0))], receivers=recs,
                  n_steps=n_steps)
+
+
+# ------------------------------------------------------------ config 4
+C4_RECEIVERS_Z = (2.0, 0.15, 13)  # first z, spacing, count (r = 0.05 m, in the mud)
+C4_ELEMENTS = (5000, 80000)
+
+
+def config4_params(n_models: int = 256, seed: int = 4) -> List[dict]:
+    """Seeded draws of the batched borehole workload: hole radius U(0.08, 0.15) m;
+    azimuthal order 0 (monopole, Ricker 8 kHz) or 1 (dipole, Ricker 3 kHz), half
+    each; 1-6 horizontal beds with vp U(2000, 5500), vs/vp U(0.4, 0.6), rho
+    U(2000, 2700) (slow formations, vs < 1500, included); a 0.01 m steel casing
+    and 0.03 m cement in 30 % of the models; GLL order 4-6; a target size of
+    5k-80k elements after AMR (log-uniform); 13 pressure receivers; 5 ms."""
+    rng = np.random.default_rng(seed)
+    orders_m = rng.permutation(np.arange(n_models) % 2)
+    out = []
+    for k in range(n_models):
+        nb = int(rng.integers(1, 7))
+        vp = rng.uniform(2000.0, 5500.0, nb)
+        vs = vp * rng.uniform(0.4, 0.6, nb)
+        rho = rng.uniform(2000.0, 2700.0, nb)
+        out.append(dict(
+            index=k,
+            m=int(orders_m[k]),
+            hole=float(rng.uniform(0.08, 0.15)),
+            casing=bool(rng.random() < 0.3),
+            order=int(rng.integers(4, 7)),
+            beds=[(float(a), float(b), float(c)) for a, b, c in zip(vp, vs, rho)],
+            bed_fracs=sorted(float(f) for f in rng.uniform(0.1, 0.9, nb - 1)),
+            target=float(np.exp(rng.uniform(np.log(C4_ELEMENTS[0]), np.log(C4_ELEMENTS[1])))),
+        ))
+    return out
+
+
+def config4_model(p: dict, zlen: float = 6.0, radius: float = 4.0, duration: float = 5e-3) -> Model:
+    """One batched borehole model: z from -1.5 m over `zlen`, formation out to `radius`."""
+    hole = p["hole"]
+    ann = [("mud", hole)] + ([("casing", hole + 0.01), ("cement", hole + 0.04)] if p["casing"] else [])
+    z0 = -1.5
+    beds = [(z0, "bed0")] + [(z0 + zlen * f, f"bed{i + 1}") for i, f in enumerate(p["bed_fracs"])]
+    b = borehole((z0, z0 + zlen), ann, formation_radius=radius, beds=beds, dz=0.08)
+    mats = {b.regions["mud"]: MUD}
+    if p["casing"]:
+        mats[b.regions["casing"]] = STEEL
+        mats[b.regions["cement"]] = CEMENT
+    for i, (vp, vs, rho) in enumerate(p["beds"]):
+        mats[b.regions[f"bed{i}"]] = Material.elastic(vp, vs, rho)
+    if p["m"] == 0:
+        f0 = 8000.0
+        src = Source("monopole", 0.0, 0.0, stf=ricker(f0))
+    else:
+        f0 = 3000.0
+        src = Source("dipole", 0.0, 0.0, (1.0, 0.0, 0.0), ricker(f0))
+    z_first, dz_rec, n_rec = C4_RECEIVERS_Z
+    recs = [Receiver(f"r{i}", 0.05, z_first + dz_rec * i, ["pressure"]) for i in range(n_rec)]
+    return Model(b.mesh, order=p["order"], f_max=0.9375 * f0, azimuthal_order=p["m"], materials=mats,
+                 boundaries={b.boundaries[n]: "absorbing" for n in ("bottom", "outer", "top")},
+                 sources=[src], receivers=recs, duration=duration)
+
+
+def n_elements(arrays: Dict[str, np.ndarray]) -> int:
+    return int(sum(v.size for k, v in arrays.items() if k.endswith(".elements")))
+
+
+def config4_calibrated(p: dict, duration: float = 5e-3, geometry: Optional[Tuple[float, float]] = None):
+    """(model, setup arrays, elements, (zlen, radius)).  Without `geometry`, the z
+    extent and formation radius are scaled (at most three setups) so the mesh
+    after AMR lands near the model's target size, inside 5k-80k elements."""
+    if geometry is not None:
+        model = config4_model(p, geometry[0], geometry[1], duration)
+        arrays = setup_arrays(model)
+        return model, arrays, n_elements(arrays), geometry
+    lo, hi = C4_ELEMENTS
+    zlen, radius = 6.0, 4.0
+    model = config4_model(p, zlen, radius, duration)
+    arrays = setup_arrays(model)
+    ne = n_elements(arrays)
+    for it in range(3):
+        if lo <= ne <= hi and (it == 2 or abs(np.log(ne / p["target"])) < 0.35):
+            break
+        s = p["target"] / ne
+        if s >= 1.0:
+            g = s ** 0.5
+            zlen, radius = min(zlen * g, 60.0), min(radius * g, 30.0)
+        else:
+            radius = max(radius * s, 0.6 + p["hole"])
+        model = config4_model(p, zlen, radius, duration)
+        arrays = setup_arrays(model)
+        ne = n_elements(arrays)
+    return model, arrays, ne, (zlen, radius)
+
+
+C4_GEOMETRY_FILE = "config4_geometry.json"
+
+
+def config4_geometry_table(n_models: int = 256, seed: int = 4) -> Optional[List[Tuple[float, float]]]:
+    """The calibrated (zlen, radius) of every model, from the table shipped with
+    the package (written by ``write_config4_geometry``), or None."""
+    import json
+    from pathlib import Path
+
+    f = Path(__file__).resolve().parent / "data" / C4_GEOMETRY_FILE
+    if not f.exists():
+        return None
+    t = json.loads(f.read_text())
+    if t.get("seed") != seed or len(t.get("geometry", [])) < n_models:
+        return None
+    return [tuple(g) for g in t["geometry"][:n_models]]
+
+
+def write_config4_geometry(n_models: int = 256, seed: int = 4) -> None:
+    """Calibrates every model of the workload and writes the geometry table."""
+    import json
+    from pathlib import Path
+
+    rows, counts = [], []
+    for p, _, _, ne, geo in config4(n_models, seed, use_table=False):
+        rows.append([round(geo[0], 6), round(geo[1], 6)])
+        counts.append(ne)
+    f = Path(__file__).resolve().parent / "data" / C4_GEOMETRY_FILE
+    f.parent.mkdir(exist_ok=True)
+    f.write_text(json.dumps({"seed": seed, "n_models": n_models, "geometry": rows, "elements": counts}) + "\n")
+
+
+def config4(n_models: int = 256, seed: int = 4, workers: Optional[int] = None, duration: float = 5e-3,
+            use_table: bool = True):
+    """Yields (params, model, setup arrays, elements, (zlen, radius)) of the
+    batched borehole workload in order; the native setups run in a thread pool."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    params = config4_params(n_models, seed)
+    table = config4_geometry_table(n_models, seed) if use_table else None
+    geos = table if table is not None else [None] * n_models
+    with ThreadPoolExecutor(max_workers=workers or max(1, min(32, os.cpu_count() or 1))) as ex:
+        results = ex.map(lambda qg: config4_calibrated(qg[0], duration, qg[1]), zip(params, geos))
+        for p, (model, arrays, ne, geo) in zip(params, results):
+            yield p, model, arrays, ne, geo

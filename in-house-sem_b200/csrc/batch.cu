@@ -12,6 +12,24 @@ static __global__ void batch_error_kernel(StepState* const* __restrict__ sts, in
   if (i < n && sts[i]->error) atomicOr(out, 1);
 }
 
+// Streamed steps: this step's amplitudes from the staged host row into each
+// solve's amplitude table (the step about to run is st->step + 1).
+static __global__ void batch_amp_scatter_kernel(const StreamSeg* __restrict__ segs, const float* __restrict__ stage) {
+  const StreamSeg& sg = segs[blockIdx.x];
+  const int32_t s = sg.st->step + 1;
+  if (s >= sg.n_amp) return;
+  for (int32_t q = threadIdx.x; q < sg.n_sources; q += blockDim.x)
+    sg.src_amp[static_cast<size_t>(q) * sg.n_amp + s] = stage[sg.amp_off + q];
+}
+
+// Streamed steps: each solve's latest sample row into the staged host row.
+static __global__ void batch_row_gather_kernel(const StreamSeg* __restrict__ segs, double* __restrict__ stage) {
+  const StreamSeg& sg = segs[blockIdx.x];
+  const int32_t sample = sg.st->step / sg.record_every;
+  for (int32_t c = threadIdx.x; c < sg.n_cols; c += blockDim.x)
+    stage[sg.col_off + c] = sample < sg.max_samples ? sg.traces[static_cast<size_t>(sample) * sg.n_cols + c] : 0.0;
+}
+
 // ------------------------------------------------------------ Solver hooks
 void Solver::batch_prepare() {
   DeviceGuard dg(device);
@@ -36,6 +54,10 @@ void Solver::batch_prepare() {
 
 void Solver::batch_collect(BatchTables& T) {
   T.states.push_back(st);
+  T.stream_segs.push_back(StreamSeg{src_amp.get(), n_amp, n_sources, T.amp_cols, trace_buf.get(), n_cols, T.row_cols,
+                                    record_every, max_samples, st});
+  T.amp_cols += n_sources;
+  T.row_cols += n_cols;
   const StepScalars sc{static_cast<float>(dt), static_cast<float>(0.5 * dt), static_cast<float>(0.5 * dt * dt),
                        energy_every};
   for (auto& t : tdom) {
@@ -306,6 +328,12 @@ void Batch::rebuild() {
   n_energy = static_cast<int32_t>(T.energy_segs.size());
   dstates.upload(T.states);
   n_states = static_cast<int32_t>(T.states.size());
+  dstream.upload(T.stream_segs);
+  n_stream = static_cast<int32_t>(T.stream_segs.size());
+  amp_cols = T.amp_cols;
+  row_cols = T.row_cols;
+  amp_stage.resize(std::max(amp_cols, 1));
+  row_stage.resize(std::max(row_cols, 1));
   CUDA_CHECK(cudaStreamSynchronize(stream));
   if (opts.use_graphs && n_states > 0) {
     cudaGraph_t g = nullptr;
@@ -334,7 +362,7 @@ void Batch::rebuild() {
   dirty = false;
 }
 
-void Batch::enqueue() {
+void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
   const int32_t nq = static_cast<int32_t>(dclasses.size());
   const int32_t nb = std::max(n_states, nq);
   batch_begin_kernel<<<ceil_div(std::max(nb, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, queues.get(), nq);
@@ -343,6 +371,7 @@ void Batch::enqueue() {
     constrained_batch_kernel<<<n_cons_items, kConsChunk, 0, stream>>>(dcons_segs.get(), dcons_items.get());
     CUDA_LAUNCH_CHECK();
   }
+  if (tiles_begin) CUDA_CHECK(cudaEventRecord(tiles_begin, stream));
   for (int32_t q = 0; q < nq; ++q) {
     const DevClass& d = dclasses[q];
     TileBatchLaunch a;
@@ -359,6 +388,7 @@ void Batch::enqueue() {
     a.stream = stream;
     tile_batch(d.ngll, a, true);
   }
+  if (tiles_end) CUDA_CHECK(cudaEventRecord(tiles_end, stream));
   // solid halos first: the fluid's coupling term reads the solid's new acceleration
   if (n_halo_items[1] > 0) {
     halo_batch_kernel<2, true><<<n_halo_items[1], kHaloChunk, 0, stream>>>(dhalo_segs[1].get(), dhalo_items[1].get());
@@ -427,6 +457,109 @@ void Batch::advance(int32_t n) {
       for (Solver* s : done) s->check_fields();
   }
   last_ms = total_ms;
+}
+
+void Batch::stream_layout(int32_t* a, int32_t* r) {
+  DeviceGuard dg(opts.device);
+  if (dirty && steps_to_next_completion() > 0) rebuild();
+  if (a) *a = steps_to_next_completion() > 0 ? amp_cols : 0;
+  if (r) *r = steps_to_next_completion() > 0 ? row_cols : 0;
+}
+
+int32_t Batch::advance_streamed(int32_t n, const float* amp_in, double* rows_out) {
+  DeviceGuard dg(opts.device);
+  INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
+  const int32_t next = steps_to_next_completion();
+  if (next == 0 || n == 0) return 0;
+  if (dirty) rebuild();
+  INSEM_REQUIRE(amp_cols == 0 || amp_in, INSEM_CUDA_ERR_INVALID, "missing source amplitudes");
+  const int32_t k = std::min(n, next);
+  CUDA_CHECK(cudaMemsetAsync(derr.get(), 0, sizeof(int32_t), stream));
+  CUDA_CHECK(cudaEventRecord(ev0, stream));
+  for (int32_t j = 0; j < k; ++j) {
+    if (amp_cols > 0) {
+      CUDA_CHECK(cudaMemcpyAsync(amp_stage.get(), amp_in + static_cast<std::size_t>(j) * amp_cols,
+                                 amp_cols * sizeof(float), cudaMemcpyHostToDevice, stream));
+      batch_amp_scatter_kernel<<<n_stream, 64, 0, stream>>>(dstream.get(), amp_stage.get());
+      CUDA_LAUNCH_CHECK();
+    }
+    if (graph) CUDA_CHECK(cudaGraphLaunch(graph, stream));
+    else enqueue();
+    if (rows_out && row_cols > 0) {
+      batch_row_gather_kernel<<<n_stream, 64, 0, stream>>>(dstream.get(), row_stage.get());
+      CUDA_LAUNCH_CHECK();
+      CUDA_CHECK(cudaMemcpyAsync(rows_out + static_cast<std::size_t>(j) * row_cols, row_stage.get(),
+                                 row_cols * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    }
+  }
+  CUDA_CHECK(cudaEventRecord(ev1, stream));
+  batch_error_kernel<<<ceil_div(std::max(n_states, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, derr.get());
+  CUDA_LAUNCH_CHECK();
+  CUDA_CHECK(cudaMemcpyAsync(herr, derr.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  CUDA_CHECK(cudaStreamSynchronize(stream));
+  float ms = 0.0f;
+  CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+  last_ms = ms;
+  point_updates = 0;
+  std::vector<Solver*> done;
+  for (std::size_t i = 0; i < members.size(); ++i) {
+    if (!members[i] || !prepared[i] || members[i]->s->remaining() <= 0) continue;
+    Solver& s = *members[i]->s;
+    s.batch_advanced(k);
+    point_updates += member_points[i] * k;
+    if (s.remaining() == 0) {
+      dirty = true;
+      done.push_back(&s);
+    }
+  }
+  INSEM_REQUIRE(!*herr, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
+  if (opts.check_finite)
+    for (Solver* s : done) s->check_fields();
+  return k;
+}
+
+void Batch::profile(int32_t n, double* tile_ms, double* step_ms) {
+  DeviceGuard dg(opts.device);
+  INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
+  const int32_t k = std::min(n, steps_to_next_completion());
+  double tt = 0.0, ts = 0.0;
+  if (k > 0) {
+    if (dirty) rebuild();
+    std::vector<cudaEvent_t> ev(4 * static_cast<std::size_t>(k));
+    for (auto& e : ev) CUDA_CHECK(cudaEventCreate(&e));
+    CUDA_CHECK(cudaMemsetAsync(derr.get(), 0, sizeof(int32_t), stream));
+    for (int32_t j = 0; j < k; ++j) {
+      CUDA_CHECK(cudaEventRecord(ev[4 * j], stream));
+      enqueue(ev[4 * j + 1], ev[4 * j + 2]);
+      CUDA_CHECK(cudaEventRecord(ev[4 * j + 3], stream));
+    }
+    batch_error_kernel<<<ceil_div(std::max(n_states, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, derr.get());
+    CUDA_LAUNCH_CHECK();
+    CUDA_CHECK(cudaMemcpyAsync(herr, derr.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+    CUDA_CHECK(cudaStreamSynchronize(stream));
+    for (int32_t j = 0; j < k; ++j) {
+      float a = 0.0f, b = 0.0f;
+      CUDA_CHECK(cudaEventElapsedTime(&a, ev[4 * j + 1], ev[4 * j + 2]));
+      CUDA_CHECK(cudaEventElapsedTime(&b, ev[4 * j], ev[4 * j + 3]));
+      tt += a;
+      ts += b;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    std::vector<Solver*> done;
+    for (std::size_t i = 0; i < members.size(); ++i) {
+      if (!members[i] || !prepared[i] || members[i]->s->remaining() <= 0) continue;
+      members[i]->s->batch_advanced(k);
+      if (members[i]->s->remaining() == 0) {
+        dirty = true;
+        done.push_back(members[i]->s.get());
+      }
+    }
+    INSEM_REQUIRE(!*herr, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
+    if (opts.check_finite)
+      for (Solver* s : done) s->check_fields();
+  }
+  if (tile_ms) *tile_ms = tt;
+  if (step_ms) *step_ms = ts;
 }
 
 void Batch::run() {
@@ -502,6 +635,28 @@ insem_cuda_solver* insem_cuda_batch_member(insem_cuda_batch* h, int32_t index) {
     out = h->b->member(index);
   });
   return out;
+}
+
+int insem_cuda_batch_advance_streamed(insem_cuda_batch* h, int32_t n, const float* amp_in, double* rows_out,
+                                      int32_t* n_done) {
+  return guarded([&] {
+    INSEM_REQUIRE(h && n_done, INSEM_CUDA_ERR_INVALID, "null argument");
+    *n_done = h->b->advance_streamed(n, amp_in, rows_out);
+  });
+}
+
+int insem_cuda_batch_stream_layout(insem_cuda_batch* h, int32_t* amp_cols, int32_t* row_cols) {
+  return guarded([&] {
+    INSEM_REQUIRE(h, INSEM_CUDA_ERR_INVALID, "null handle");
+    h->b->stream_layout(amp_cols, row_cols);
+  });
+}
+
+int insem_cuda_batch_profile(insem_cuda_batch* h, int32_t n, double* tile_ms, double* step_ms) {
+  return guarded([&] {
+    INSEM_REQUIRE(h, INSEM_CUDA_ERR_INVALID, "null handle");
+    h->b->profile(n, tile_ms, step_ms);
+  });
 }
 
 int32_t insem_cuda_batch_size(const insem_cuda_batch* h) { return h ? h->b->size() : 0; }

@@ -26,6 +26,16 @@
 
 namespace insem_b200 {
 
+// Streamed batched steps: where each solve's amplitudes and sample columns sit
+// in the per-step host rows.
+struct StreamSeg {
+  float* src_amp;        // [n_sources][n_amp] amplitude table of the solve
+  int32_t n_amp, n_sources, amp_off;
+  const double* traces;  // [max_samples][n_cols]
+  int32_t n_cols, col_off, record_every, max_samples;
+  const StepState* st;
+};
+
 struct TileClass {
   int ngll = 0, kind = 0, m = 0, ncomp = 0;
   bool elastic = false;
@@ -45,6 +55,8 @@ struct BatchTables {
   std::vector<int2> pv_items, rec_items;
   std::vector<EnergySeg> energy_segs;
   std::vector<StepState*> states;
+  std::vector<StreamSeg> stream_segs;
+  int32_t amp_cols = 0, row_cols = 0;
 };
 
 class Batch {
@@ -62,6 +74,16 @@ class Batch {
   void advance(int32_t n);
   // Steps until every solve is complete.
   void run();
+  // Up to n steps (stopping at the next completion) with per-step host I/O:
+  // amp_in[step][amp_cols] are the active solves' source amplitudes (in index
+  // order, each solve's sources in order), rows_out[step][row_cols] their
+  // latest sample rows.  Returns the steps done.
+  int32_t advance_streamed(int32_t n, const float* amp_in, double* rows_out);
+  // Column counts of the streamed rows for the current composition.
+  void stream_layout(int32_t* amp_cols, int32_t* row_cols);
+  // n steps with plain launches and CUDA events around the tile launches of
+  // every step: device ms of the tile launches and of the whole steps.
+  void profile(int32_t n, double* tile_ms, double* step_ms);
   // Frees a solve (its index stays unused).
   void remove(int32_t index);
   insem_cuda_solver* member(int32_t index);
@@ -76,7 +98,7 @@ class Batch {
 
  private:
   void rebuild();
-  void enqueue();
+  void enqueue(cudaEvent_t tiles_begin = nullptr, cudaEvent_t tiles_end = nullptr);
 
   struct DevClass {
     int ngll = 0, kind = 0, m = 0;
@@ -111,6 +133,10 @@ class Batch {
   int32_t n_energy = 0;
   DeviceBuffer<StepState*> dstates;
   int32_t n_states = 0;
+  DeviceBuffer<StreamSeg> dstream;
+  int32_t n_stream = 0, amp_cols = 0, row_cols = 0;
+  DeviceBuffer<float> amp_stage;
+  DeviceBuffer<double> row_stage;
   DeviceBuffer<int32_t> derr;
   int32_t* herr = nullptr;  // pinned
   std::vector<int64_t> member_points;

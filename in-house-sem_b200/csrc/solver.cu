@@ -66,6 +66,10 @@ void DeviceDomainData::upload(const insem_cuda_domain& d, const insem_cuda_basis
   }
   host_zero = z;
   zero_idx.upload(z);
+}
+
+void DeviceDomainData::alloc_fields() {
+  if (fields_ready) return;
   const std::size_t nf = static_cast<std::size_t>(ncomp) * ng;
   u.resize(nf);
   v.resize(nf);
@@ -77,6 +81,7 @@ void DeviceDomainData::upload(const insem_cuda_domain& d, const insem_cuda_basis
   a.zero();
   f.zero();
   f_local.zero();
+  fields_ready = true;
 }
 
 Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool setup_only) {
@@ -129,6 +134,10 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
     hs.kin_c = dt * dt / 8.0;
     CUDA_CHECK(cudaMemcpy(st, &hs, sizeof(hs), cudaMemcpyHostToDevice));
   }
+  // the two-pass path's global fields and element-local forces; the tiled
+  // path keeps its own fields and allocates these only for internal_forces()
+  if (setup_only || opts.path == 1)
+    for (auto& d : domains) d.alloc_fields();
   if (!setup_only && opts.path != 1) build_tiled(p);
   CUDA_CHECK(cudaStreamSynchronize(nullptr));
   CUDA_CHECK(cudaDeviceSynchronize());
@@ -301,6 +310,7 @@ AllFields Solver::fields_view() {
 }
 
 void Solver::internal_forces(DeviceDomainData& d, const float* u_global, float* f_global) {
+  d.alloc_fields();
   for (const DeviceBlock& b : d.blocks) {
     ElementLaunch a;
     a.basis = basis.view();
@@ -391,6 +401,7 @@ double Solver::reduce_partials() {
 // with x ~ U(-1, 1) from mt19937(12345), Rayleigh quotients in double.
 double Solver::stable_dt() {
   DeviceGuard dg(device);
+  for (auto& d : domains) d.alloc_fields();
   double lambda = 0.0;
   std::mt19937 rng(12345);
   std::uniform_real_distribution<double> dist(-1.0, 1.0);
@@ -557,9 +568,10 @@ void Solver::set_state(int32_t medium, const double* u_in, const double* v_in) {
     fv[i] = static_cast<float>(v_in[i]);
   }
   for (int64_t z : d.host_zero) fu[z] = fv[z] = 0.0f;
-  CUDA_CHECK(cudaMemcpy(d.u.get(), fu.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-  CUDA_CHECK(cudaMemcpy(d.v.get(), fv.data(), n * sizeof(float), cudaMemcpyHostToDevice));
-  if (tiled) {
+  if (!tiled) {
+    CUDA_CHECK(cudaMemcpy(d.u.get(), fu.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpy(d.v.get(), fv.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  } else {
     TiledDomain& t = tdom[di];
     const std::size_t nd = static_cast<std::size_t>(d.ncomp) * t.ng;
     std::vector<float> pu(nd, 0.0f), pv(nd, 0.0f);
@@ -701,7 +713,7 @@ void Solver::copy_state(int32_t di, double* u_out, double* v_out, double* a_out)
   INSEM_REQUIRE(di >= 0 && di < static_cast<int32_t>(domains.size()), INSEM_CUDA_ERR_INVALID, "domain out of range");
   auto& d = domains[di];
   CUDA_CHECK(cudaStreamSynchronize(stream));
-  if (tiled && initialized) {
+  if (tiled) {  // before the first step: the set state, a = 0
     TiledDomain& t = tdom[di];
     auto conv = [&](const float* dev, double* out) {
       if (!out) return;
@@ -1100,6 +1112,25 @@ int insem_cuda_solver_internal_forces(insem_cuda_solver* h, int32_t domain, cons
     s.internal_forces(d, du.get(), df.get());
     CUDA_CHECK(cudaStreamSynchronize(s.stream));
     CUDA_CHECK(cudaMemcpy(f, df.get(), n * sizeof(float), cudaMemcpyDeviceToHost));
+  });
+}
+
+int insem_cuda_solver_point_classes(const insem_cuda_solver* h, int32_t domain, int32_t* n_tile_points,
+                                    int32_t* n_halo_points) {
+  return guarded([&] {
+    INSEM_REQUIRE(h, INSEM_CUDA_ERR_INVALID, "null handle");
+    const Solver& s = *h->s;
+    INSEM_REQUIRE(domain >= 0 && domain < static_cast<int32_t>(s.domains.size()), INSEM_CUDA_ERR_INVALID,
+                  "domain out of range");
+    int32_t nt = 0, nh = 0;
+    if (s.tiled) {
+      nh = s.tiled_halo_points(domain);
+      nt = s.domains[domain].ng - nh;
+    } else {
+      nh = s.domains[domain].ng;
+    }
+    if (n_tile_points) *n_tile_points = nt;
+    if (n_halo_points) *n_halo_points = nh;
   });
 }
 

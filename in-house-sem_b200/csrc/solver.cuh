@@ -24,7 +24,9 @@ struct DeviceDomainData {
   DeviceBuffer<float> absorbing_coef;
   std::vector<int64_t> host_zero;   // Dirichlet and axis entries (component * ng + point)
   DeviceBuffer<int64_t> zero_idx;
-  DeviceBuffer<float> u, v, a, f, f_local;
+  DeviceBuffer<float> u, v, a, f, f_local;  // two-pass path only (alloc_fields)
+  bool fields_ready = false;
+  void alloc_fields();
 
   void upload(const insem_cuda_domain& d, const insem_cuda_basis& basis);
 };
@@ -152,6 +154,8 @@ class Solver {
   void batch_advanced(int32_t k);
   // NaN/Inf check of the current fields (throws INSEM_CUDA_ERR_NONFINITE).
   void check_fields();
+  // Points of a domain finished by the halo kernel (the rest by their tile).
+  int32_t tiled_halo_points(int di) const { return tdom[di].n_halo; }
 };
 
 }  // namespace insem_b200

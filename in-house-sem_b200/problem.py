@@ -163,6 +163,22 @@ class ProblemData:
                 total += b.n_elements * (4 * npe + metric + coef)
         return int(total)
 
+    def algorithmic_bytes_split(self, tile_points) -> tuple:
+        """(bytes of the tile kernels, bytes of the halo kernels) of one step: the
+        element terms and the points finished in their tile, against the points
+        finished by the halo kernel; tile_points[d] per domain."""
+        npe = self.ngll * self.ngll
+        tile = halo = 0
+        for d, nt in zip(self.domains, tile_points):
+            per_point = 16 * d.ncomp + 4
+            tile += nt * per_point
+            halo += (d.n_global - nt) * per_point
+            coef = (8 if d.medium == N.ELASTIC else 4) * npe
+            for b in d.blocks:
+                metric = {N.RECT: 12, N.AFFINE: 20, N.CURVED: 20 * npe, N.AXISYM: 32 * npe}[b.kind]
+                tile += b.n_elements * (4 * npe + metric + coef)
+        return int(tile), int(halo)
+
     # ------------------------------------------------------------- storage
     @staticmethod
     def from_npz(z, prefix: str = "problem.") -> "ProblemData":

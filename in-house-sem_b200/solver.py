@@ -97,6 +97,17 @@ class Solver:
     def kernels_per_step(self) -> int:
         return int(N.lib().insem_cuda_solver_kernels_per_step(self._h))
 
+    def point_classes(self, domain: int) -> Tuple[int, int]:
+        """(points finished in their tile, points finished by the halo kernel)."""
+        nt, nh = C.c_int32(), C.c_int32()
+        N.check(N.lib().insem_cuda_solver_point_classes(self._h, int(domain), C.byref(nt), C.byref(nh)))
+        return nt.value, nh.value
+
+    def algorithmic_bytes_split(self) -> Tuple[int, int]:
+        """(tile-kernel bytes, halo-kernel bytes) of one step (the roofline's split)."""
+        return self.problem.algorithmic_bytes_split(
+            [self.point_classes(i)[0] for i in range(len(self.problem.domains))])
+
     # ------------------------------------------------------------- state
     def _domain(self, medium: str) -> int:
         di = self.problem.domain_index(medium)

@@ -285,6 +285,10 @@ int insem_cuda_solver_advance_streamed(insem_cuda_solver* h, int32_t n, const fl
 int32_t insem_cuda_solver_n_columns(const insem_cuda_solver* h);
 /* Kernel launches of one captured step (the step graph's kernel nodes). */
 int32_t insem_cuda_solver_kernels_per_step(insem_cuda_solver* h);
+/* Points of a domain finished inside their tile's kernel and by the halo
+ * kernel (the roofline's split of the step's bytes). */
+int insem_cuda_solver_point_classes(const insem_cuda_solver* h, int32_t domain, int32_t* n_tile_points,
+                                    int32_t* n_halo_points);
 
 /* ------------------------------------------------------------ stable dt */
 /* Power iteration for lambda_max(M^-1 K) with the reference's seeds and
@@ -317,6 +321,21 @@ int insem_cuda_batch_run(insem_cuda_batch* h);
 int insem_cuda_batch_remove(insem_cuda_batch* h, int32_t index);
 /* Borrowed handle of member `index` (NULL and an error message if there is none). */
 insem_cuda_solver* insem_cuda_batch_member(insem_cuda_batch* h, int32_t index);
+/* Streamed batched steps (end-to-end serving form): up to n steps, stopping
+ * at the next member completion; *n_done is the number done.  Per step it
+ * takes amp_in[step][amp_cols], the source amplitudes of the active members
+ * (index order, each member's sources in order, FP32 as the reference casts
+ * them), and writes rows_out[step][row_cols], each active member's latest
+ * sample row (its columns as insem_cuda_solver_n_columns lays them out); one
+ * host-to-device and one device-to-host copy per step.  rows_out may be NULL. */
+int insem_cuda_batch_advance_streamed(insem_cuda_batch* h, int32_t n, const float* amp_in, double* rows_out,
+                                      int32_t* n_done);
+/* n steps with plain launches and CUDA events around each step's tile
+ * launches (stops at the next completion): device ms of the tile launches
+ * and of the whole steps. */
+int insem_cuda_batch_profile(insem_cuda_batch* h, int32_t n, double* tile_ms, double* step_ms);
+/* amp_cols and row_cols of the current composition (0 when nothing is running). */
+int insem_cuda_batch_stream_layout(insem_cuda_batch* h, int32_t* amp_cols, int32_t* row_cols);
 int32_t insem_cuda_batch_size(const insem_cuda_batch* h);
 int32_t insem_cuda_batch_active(const insem_cuda_batch* h);
 /* Steps until the next member completes (0 when none is running). */

@@ -114,3 +114,44 @@ def test_adopted_solver_continues_bitwise(pkg):
         m = b.adopt(s)
         b.run()
         _check_golden("lay", prob, m, z)
+
+
+def test_batch_streamed_rows_match_reference(pkg):
+    """Streamed batched steps (amplitudes in, sample rows out, every step) give
+    the reference's samples, member by member, across completions."""
+    from insem_b200 import Batch
+    from insem_b200.stf import amplitudes
+
+    with Batch() as b:
+        ref = {}
+        for case in ("c1", "lay", "bh1"):
+            z = golden(case)
+            prob = pkg.ProblemData.from_npz(z)
+            m = b.add(prob)
+            _init_state(m, prob, z)
+            full = np.concatenate([z[f"run.trace.{n}.{q}"] for n, q in prob.trace_list()], axis=1)
+            ref[m.index] = (prob, full)
+        b.advance(3)
+        checked = 0
+        while b.active:
+            amp_cols, row_cols = b.stream_layout()
+            act = b.active_members()
+            k = min(b.steps_to_next_completion, 37)
+            first = {m.index: m.step + 1 for m in act}
+            amp = np.concatenate([amplitudes(ref[m.index][0], first[m.index], k) for m in act], axis=1)
+            amp = np.ascontiguousarray(amp, np.float32)
+            assert amp.shape[1] == amp_cols
+            rows = np.zeros((k, row_cols))
+            got = b.advance_streamed(k, amp, rows)
+            assert got == k
+            col = 0
+            for m in act:
+                prob, full = ref[m.index]
+                nc = full.shape[1]
+                for j in range(got):
+                    s = first[m.index] + j
+                    assert np.array_equal(rows[j, col:col + nc], full[s // prob.record_every]), (m.index, s)
+                    checked += 1
+                col += nc
+            assert col == row_cols
+        assert checked > 0
