@@ -298,18 +298,24 @@ def bench_config3(args, world, rank, device, pg, headline: bool) -> dict:
 
 
 def build_config4(args, device):
-    """The batched borehole models as (params, problem, solver); setups in a thread pool."""
+    """The batched borehole models as (params, problem, solver): setups in a
+    thread pool, the tile autotuner on the largest model of each tile class,
+    then the solvers."""
     import __graft_entry__ as entry
 
     pkg = entry.load_package()
+    from insem_b200 import autotune
     from insem_b200 import cases as K
 
-    out = []
+    probs = []
     for p, model, arrays, ne, geo in K.config4(args.models, 4):
-        prob = K.build_from_arrays(model, arrays, device=device)
+        probs.append((p, K.build_from_arrays(model, arrays, device=device)))
         del arrays
-        out.append((p, prob, pkg.Solver(prob, device=device, use_graphs=not args.no_graphs)))
-    return out
+    t0 = time.perf_counter()
+    table = None if args.no_autotune else autotune.tune([q for _, q in probs], device=device)
+    tune_s = time.perf_counter() - t0
+    out = [(p, prob, pkg.Solver(prob, device=device, use_graphs=not args.no_graphs)) for p, prob in probs]
+    return out, {"classes": autotune.summary(table), "seconds": round(tune_s, 1)} if table else None
 
 
 def bench_config4(args, world, rank, device, pg) -> dict:
@@ -321,7 +327,7 @@ def bench_config4(args, world, rank, device, pg) -> dict:
     from insem_b200.stf import amplitudes
 
     t0 = time.perf_counter()
-    models = build_config4(args, device)
+    models, tuned = build_config4(args, device)
     setup_s = time.perf_counter() - t0
     points = sum(prob.n_global_total() for _, prob, _ in models)
     elements = sum(prob.n_elements_total() for _, prob, _ in models)
@@ -400,6 +406,7 @@ def bench_config4(args, world, rank, device, pg) -> dict:
         "gpu_launches": (kps or 0) * args.steps,
         "kernels_per_step": kps,
         "clocks": clocks.summary(),
+        "autotune": tuned,
     }
     batch.close()
     return line
@@ -457,6 +464,7 @@ def main():
     ap.add_argument("--nx", type=int, default=1024, help="config3 elements per side")
     ap.add_argument("--config3-steps", type=int, default=200, help="steps of the config3 sub-run")
     ap.add_argument("--no-config3", action="store_true", help="skip the config3 sub-run")
+    ap.add_argument("--no-autotune", action="store_true", help="batched workload: keep the default tile sizes")
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the streamed end-to-end run")

@@ -89,6 +89,7 @@ void Solver::batch_collect(BatchTables& T) {
       c.m = m;
       c.ncomp = t.ncomp;
       c.elastic = el;
+      c.te = std::max(c.te, t.te);
       c.tp_cap = std::max(c.tp_cap, t.tp_cap);
       c.nc_cap = std::max(c.nc_cap, t.nc_cap);
       const int32_t seg = static_cast<int32_t>(c.segs.size());
@@ -298,8 +299,10 @@ void Batch::rebuild() {
     d.segs.upload(c.segs);
     d.items.upload(c.items);
     d.n_items = static_cast<int32_t>(c.items.size());
-    d.L = TileLayout::make(c.ngll, c.ncomp, c.kind, c.elastic, tile_elements(c.ngll), c.tp_cap, c.nc_cap);
+    d.te = c.te;
+    d.L = TileLayout::make(c.ngll, c.ncomp, c.kind, c.elastic, c.te, c.tp_cap, c.nc_cap);
     TileBatchLaunch a;
+    a.te = c.te;
     a.kind = c.kind;
     a.m = c.m;
     a.elastic = c.elastic;
@@ -382,6 +385,7 @@ void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
     a.items = d.items.get();
     a.n_items = d.n_items;
     a.queue = queues.get() + q;
+    a.te = d.te;
     a.L = d.L;
     a.smem = d.L.total;
     a.grid = d.grid;

@@ -39,7 +39,7 @@ struct StreamSeg {
 struct TileClass {
   int ngll = 0, kind = 0, m = 0, ncomp = 0;
   bool elastic = false;
-  int tp_cap = 0, nc_cap = 0;  // largest tile of the class
+  int tp_cap = 0, nc_cap = 0, te = 0;  // largest tile of the class
   std::vector<TileSeg> segs;
   std::vector<int2> items;
 };
@@ -106,6 +106,7 @@ class Batch {
     DeviceBuffer<TileSeg> segs;
     DeviceBuffer<int2> items;
     int32_t n_items = 0;
+    int te = 0;
     TileLayout L{};
     int grid = 0;
   };

@@ -743,7 +743,6 @@ void Solver::build_tiled(const insem_cuda_problem& p) {
   const std::size_t npe = static_cast<std::size_t>(ngll) * ngll;
   set_constant_basis(ngll, host_vec(p.basis.D, npe), p.basis.Dj ? host_vec(p.basis.Dj, npe) : std::vector<float>{},
                      host_vec(p.basis.w2, npe));
-  const int te = opts.tile_elements > 0 ? std::min(opts.tile_elements, tile_elements(ngll)) : tile_elements(ngll);
   const auto fp = host_vec(p.coupling.fluid_points, n_cpl), sp = host_vec(p.coupling.solid_points, n_cpl);
   tdom.resize(domains.size());
   for (std::size_t di = 0; di < domains.size(); ++di) {
@@ -766,6 +765,18 @@ void Solver::build_tiled(const insem_cuda_problem& p) {
     for (int r = 0; r < p.n_receivers; ++r)
       if (p.receivers[r].domain == static_cast<int>(di))
         for (int32_t g : host_vec(p.receivers[r].points, p.receivers[r].n_points)) terms.receivers.push_back(g);
+    // tile size by the domain's dominant element kind
+    std::map<int, int64_t> per_kind;
+    for (int b = 0; b < d.n_blocks; ++b) per_kind[d.blocks[b].kind] += d.blocks[b].n_elements;
+    int kind = INSEM_RECT;
+    int64_t most = -1;
+    for (const auto& kv : per_kind)
+      if (kv.second > most) {
+        most = kv.second;
+        kind = kv.first;
+      }
+    const int te = choose_tile_elements(ngll, kind, d.medium == INSEM_ELASTIC, kind == INSEM_AXISYM ? d.azimuthal_order : 0,
+                                        d.ncomp, opts.tile_elements);
     tdom[di].build(d, ngll, te, terms,
                    host_vec(d.absorbing_coef, static_cast<std::size_t>(d.n_absorbing) * d.ncomp * d.ncomp));
   }
@@ -1113,6 +1124,29 @@ int insem_cuda_solver_internal_forces(insem_cuda_solver* h, int32_t domain, cons
     CUDA_CHECK(cudaStreamSynchronize(s.stream));
     CUDA_CHECK(cudaMemcpy(f, df.get(), n * sizeof(float), cudaMemcpyDeviceToHost));
   });
+}
+
+int insem_cuda_set_tile_elements(int32_t ngll, int32_t kind, int32_t medium, int32_t azimuthal_order,
+                                 int32_t tile_elements) {
+  return guarded([&] {
+    INSEM_REQUIRE(kind >= INSEM_RECT && kind <= INSEM_AXISYM, INSEM_CUDA_ERR_INVALID, "unknown geometry kind");
+    INSEM_REQUIRE(azimuthal_order == 0 || (azimuthal_order == 1 && kind == INSEM_AXISYM), INSEM_CUDA_ERR_INVALID,
+                  "azimuthal order 1 needs the axisymmetric kind");
+    set_tile_elements(ngll, kind, medium == INSEM_ELASTIC, azimuthal_order, tile_elements);
+  });
+}
+
+int32_t insem_cuda_tile_elements(int32_t ngll, int32_t kind, int32_t medium, int32_t azimuthal_order, int32_t ncomp) {
+  int32_t out = 0;
+  guarded([&] {
+    out = choose_tile_elements(ngll, kind, medium == INSEM_ELASTIC, kind == INSEM_AXISYM ? azimuthal_order : 0, ncomp, 0);
+  });
+  return out;
+}
+
+int32_t insem_cuda_solver_tile_elements(const insem_cuda_solver* h, int32_t domain) {
+  if (!h || !h->s->tiled || domain < 0 || domain >= static_cast<int32_t>(h->s->domains.size())) return 0;
+  return h->s->tiled_tile_elements(domain);
 }
 
 int insem_cuda_solver_point_classes(const insem_cuda_solver* h, int32_t domain, int32_t* n_tile_points,

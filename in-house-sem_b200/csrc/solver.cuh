@@ -156,6 +156,7 @@ class Solver {
   void check_fields();
   // Points of a domain finished by the halo kernel (the rest by their tile).
   int32_t tiled_halo_points(int di) const { return tdom[di].n_halo; }
+  int32_t tiled_tile_elements(int di) const { return tdom[di].te; }
 };
 
 }  // namespace insem_b200

@@ -84,13 +84,18 @@ struct StepScalars {
   int32_t energy_every;
 };
 
+// Tile elements are chosen per domain at run time (te <= TE, one thread per
+// element column).  CTAs are whole warps: te x NG threads rounded up to a
+// multiple of 32 (the extra threads have no element and only take part in the
+// strided loops, the barriers and the warp reductions).
 template <int NG>
 struct TileCfg {
   static constexpr int NPE = NG * NG;
   static constexpr int TE = (256 / NG) > 64 ? 64 : (256 / NG);  // elements per tile (max)
-  static constexpr int THREADS = TE * NG;
+  static constexpr int THREADS = (TE * NG + 31) / 32 * 32;       // threads per CTA (max)
   static constexpr int ROW = (NG + 1) & ~1;                      // padded row stride (floats)
 };
+__host__ __device__ constexpr int tile_threads(int te, int ng) { return (te * ng + 31) / 32 * 32; }
 
 __device__ __forceinline__ float cbasis(int ng, int which, int idx) { return c_basis[ng - 2][which][idx]; }
 
@@ -278,6 +283,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 
   const TileHdr th = td.tiles[tile];
   const int tid = threadIdx.x;
+  const int nthreads = blockDim.x;  // (tile elements) x NG
   const int mode = st->mode;
   const int32_t step = st->step;
   const bool energy = (mode == kModeInit) ? (sc.energy_every > 0) : (sc.energy_every > 0 && step % sc.energy_every == 0);
@@ -308,7 +314,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     }
   }
   // halo tile points, gathered while the bulk copies are in flight
-  for (int t = tid; t < th.ntp - th.nc; t += Cfg::THREADS) {
+  for (int t = tid; t < th.ntp - th.nc; t += nthreads) {
     const int32_t g = td.halo_tp[th.hl_off + t];
 #pragma unroll
     for (int c = 0; c < NC; ++c) tu[c * tp_cap + nc4 + t] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
@@ -351,7 +357,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       }
     }
   }
-  for (int q = tid; q < th.ncs; q += Cfg::THREADS) {
+  for (int q = tid; q < th.ncs; q += nthreads) {
     const int32_t ls = td.cs_slot[th.cs_off + q];
     const int32_t ci = td.cs_idx[th.cs_off + q];
     const int e = ls / NPE, k = ls - e * NPE;
@@ -467,7 +473,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   }
 
   // 6. halo contributions out (hbuf order = ascending slot order within the tile)
-  for (int q = tid; q < th.nhs; q += Cfg::THREADS) {
+  for (int q = tid; q < th.nhs; q += nthreads) {
     const int32_t ls = td.hs_slot[th.hs_off + q];
     const int e = ls / NPE, k = ls - e * NPE;
 #pragma unroll
@@ -477,7 +483,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 
   // 7. complete points: a = f / M, corrector, predictor; energy partials
   double kin = 0.0, pot = 0.0;
-  for (int t = tid; t < th.nc; t += Cfg::THREADS) {
+  for (int t = tid; t < th.nc; t += nthreads) {
     const int32_t g = th.cbeg + t;
     const float im = s_im[t];
 #pragma unroll
@@ -515,7 +521,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     __syncthreads();
     if (tid == 0) {
       double k2 = 0.0, p2 = 0.0;
-      for (int q = 0; q < (Cfg::THREADS + 31) / 32; ++q) {
+      for (int q = 0; q < (nthreads + 31) / 32; ++q) {
         k2 = dadd(k2, wk[q]);
         p2 = dadd(p2, wp[q]);
       }

@@ -15,6 +15,9 @@
 //   5. halo slots write to a halo buffer whose entries each halo point sums
 //      through a CSR in ascending slot order (weights of constrained maps kept).
 #include <algorithm>
+#include <cmath>
+#include <map>
+#include <mutex>
 #include <numeric>
 
 #include "tiled_path.cuh"
@@ -81,6 +84,58 @@ void launch_tiles(int ngll, const TileLaunch& a) {
     case 9: launch_tiles_ng9(a); break;
     default: check_ngll(ngll);
   }
+}
+
+namespace {
+std::mutex g_tile_mutex;
+std::map<int, int> g_tile_table;  // key (ngll, kind, elastic, m) -> elements per tile
+int tile_key(int ngll, int kind, bool elastic, int m) { return ((ngll * 4 + kind) * 2 + (elastic ? 1 : 0)) * 2 + m; }
+}  // namespace
+
+void set_tile_elements(int ngll, int kind, bool elastic, int m, int te) {
+  check_ngll(ngll);
+  INSEM_REQUIRE(te <= tile_elements(ngll), INSEM_CUDA_ERR_INVALID, "more tile elements than the kernel takes");
+  std::lock_guard<std::mutex> lk(g_tile_mutex);
+  if (te <= 0) g_tile_table.erase(tile_key(ngll, kind, elastic, m));
+  else g_tile_table[tile_key(ngll, kind, elastic, m)] = te;
+}
+
+int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp) {
+  const int te_max = tile_elements(ngll);
+  const int q = ngll - 1;
+  double best = -1.0;
+  int best_te = te_max;
+  for (int te = te_max; te >= 1; --te) {
+    if (tile_threads(te, ngll) < 64 && te < te_max) break;
+    // tile points: interior (q^2 per element) plus the patch's perimeter
+    const int side = static_cast<int>(std::ceil(std::sqrt(static_cast<double>(te))));
+    const int nc = te * q * q;
+    const int tp = nc + 4 * side * q + 4;
+    const TileLayout L = TileLayout::make(ngll, ncomp, kind, elastic, te, (tp + 3) & ~3, (nc + 3) & ~3);
+    const int ctas = std::min({(228 * 1024) / (static_cast<int>(L.total) + 1024), 2048 / tile_threads(te, ngll), 32});
+    if (ctas < 1) continue;
+    const double halo = static_cast<double>(tp - nc) / tp;                 // points shared with other tiles
+    const double overlap = ctas >= 3 ? 1.0 : ctas == 2 ? 0.9 : 0.6;       // copies of one tile under another's math
+    const double lanes = static_cast<double>(te * ngll) / tile_threads(te, ngll);  // threads with an element column
+    const double score = ctas * te * (1.0 - 0.5 * halo) * overlap * (0.8 + 0.2 * lanes);
+    if (score > best + 1e-9) {
+      best = score;
+      best_te = te;
+    }
+  }
+  (void)m;
+  return best_te;
+}
+
+int choose_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp, int requested) {
+  const int te_max = tile_elements(ngll);
+  if (requested > 0) return std::min(requested, te_max);
+  {
+    std::lock_guard<std::mutex> lk(g_tile_mutex);
+    const auto it = g_tile_table.find(tile_key(ngll, kind, elastic, m));
+    if (it != g_tile_table.end()) return std::min(it->second, te_max);
+  }
+  return analytic_tile_elements(ngll, kind, elastic, m, ncomp);
 }
 
 int tile_batch(int ngll, const TileBatchLaunch& a, bool launch) {
@@ -160,6 +215,7 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
   medium = d.medium;
   ncomp = d.ncomp;
   m = d.azimuthal_order;
+  this->te = te;
   ng = d.dofs.n_global;  // reference count while building; the padded stride at the end
   ng_ref = ng;
   npe = ngll * ngll;

@@ -29,6 +29,7 @@ class TiledDomain {
   // reference's point count.  Halo points are [n_complete, n_complete + n_halo).
   int medium = 0, ncomp = 1, m = 0, ng = 0, ng_ref = 0, npe = 0, n_elements = 0;
   int n_complete = 0, n_halo = 0, n_tiles = 0, tp_cap = 0, nc_cap = 0, n_hbuf = 0, n_cslots = 0;
+  int te = 0;  // elements per tile (CTAs of tile_threads(te, ngll) threads)
   bool weighted = false;
   std::vector<int32_t> perm;  // reference point -> device point
   struct BlockTiles {
@@ -77,7 +78,13 @@ void launch_tiles_ng7(const TileLaunch&);
 void launch_tiles_ng8(const TileLaunch&);
 void launch_tiles_ng9(const TileLaunch&);
 void launch_tiles(int ngll, const TileLaunch& a);
-int tile_elements(int ngll);  // TileCfg<NG>::TE
+int tile_elements(int ngll);  // TileCfg<NG>::TE (the largest tile)
+// Elements per tile of a domain: `requested` if > 0, else a registered entry
+// (set_tile_elements, e.g. from the autotuner), else the analytic choice that
+// keeps the most elements resident per SM with several CTAs per SM.
+int choose_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp, int requested);
+void set_tile_elements(int ngll, int kind, bool elastic, int m, int te);  // te <= 0 clears the entry
+int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp);
 // Uploads the GLL / GLJ basis of one ngll to constant memory (must agree with earlier uploads).
 void set_constant_basis(int ngll, const std::vector<float>& D, const std::vector<float>& Dj,
                         const std::vector<float>& w2);
@@ -91,6 +98,7 @@ struct TileBatchLaunch {
   const int2* items = nullptr;
   int32_t n_items = 0;
   int32_t* queue = nullptr;
+  int te = 0;      // elements per tile of the class (CTA size tile_threads(te, ngll))
   TileLayout L{};  // the class layout; its total is the dynamic shared memory
   uint32_t smem = 0;
   int grid = 0;
@@ -115,10 +123,11 @@ int tile_batch_cfg(const TileBatchLaunch& a, bool launch) {
     if (!launch) {
       CUDA_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(a.smem)));
       int nb = 0;
-      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, TileCfg<NG>::THREADS, a.smem));
+      CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, tile_threads(a.te, NG), a.smem));
       return nb;
     }
-    kernel<<<a.grid, TileCfg<NG>::THREADS, a.smem, a.stream>>>(a.segs, a.items, a.n_items, a.queue, a.L);
+    INSEM_REQUIRE(a.te >= 1 && a.te <= TileCfg<NG>::TE, INSEM_CUDA_ERR_INVALID, "tile elements out of range");
+    kernel<<<a.grid, tile_threads(a.te, NG), a.smem, a.stream>>>(a.segs, a.items, a.n_items, a.queue, a.L);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess)
       throw Error(INSEM_CUDA_ERR_CUDA, "batched tile kernel launch (ngll " + std::to_string(NG) + ", kind " +
@@ -149,7 +158,8 @@ void launch_tiles_cfg(const TileLaunch& a) {
   const auto& b = d.blocks[a.block];
   if (b.ntiles == 0) return;
   auto go = [&](auto kernel, int nc) {
-    const TileLayout L = TileLayout::make(NG, nc, b.kind, a.elastic, TileCfg<NG>::TE, d.tp_cap, d.nc_cap);
+    INSEM_REQUIRE(d.te >= 1 && d.te <= TileCfg<NG>::TE, INSEM_CUDA_ERR_INVALID, "tile elements out of range");
+    const TileLayout L = TileLayout::make(NG, nc, b.kind, a.elastic, d.te, d.tp_cap, d.nc_cap);
     const size_t smem = L.total;
     // Opt in to this launch's dynamic shared memory (outside stream capture;
     // the first launch of every tile kernel happens in the uncaptured initial step).
@@ -160,12 +170,12 @@ void launch_tiles_cfg(const TileLaunch& a) {
     INSEM_REQUIRE(smem <= 227 * 1024, INSEM_CUDA_ERR_UNSUPPORTED, "tile needs too much shared memory");
     TiledDev td = d.view(a.parity);
     td.sdesc += static_cast<size_t>(b.e_off) * point_stride<NG * NG>();
-    kernel<<<b.ntiles, TileCfg<NG>::THREADS, smem, a.stream>>>(b.view(), td, a.sc, a.st, a.epartial, b.tile0, L);
+    kernel<<<b.ntiles, tile_threads(d.te, NG), smem, a.stream>>>(b.view(), td, a.sc, a.st, a.epartial, b.tile0, L);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess)
       throw Error(INSEM_CUDA_ERR_CUDA, "tile kernel launch (ngll " + std::to_string(NG) + ", kind " +
                                            std::to_string(b.kind) + ", tiles " + std::to_string(b.ntiles) +
-                                           ", threads " + std::to_string(TileCfg<NG>::THREADS) + ", smem " +
+                                           ", threads " + std::to_string(tile_threads(d.te, NG)) + ", smem " +
                                            std::to_string(smem) + "): " + cudaGetErrorString(err));
   };
   if (b.kind == INSEM_AXISYM) {

@@ -150,6 +150,9 @@ def lib() -> C.CDLL:
             "insem_cuda_batch_stream_layout": (C.c_int, [vp, i32p, i32p]),
             "insem_cuda_batch_profile": (C.c_int, [vp, C.c_int32, f64p, f64p]),
             "insem_cuda_solver_point_classes": (C.c_int, [vp, C.c_int32, i32p, i32p]),
+            "insem_cuda_set_tile_elements": (C.c_int, [C.c_int32] * 5),
+            "insem_cuda_tile_elements": (C.c_int32, [C.c_int32] * 5),
+            "insem_cuda_solver_tile_elements": (C.c_int32, [vp, C.c_int32]),
             "insem_cuda_batch_size": (C.c_int32, [vp]),
             "insem_cuda_batch_active": (C.c_int32, [vp]),
             "insem_cuda_batch_steps_to_next_completion": (C.c_int32, [vp]),

@@ -285,6 +285,18 @@ int insem_cuda_solver_advance_streamed(insem_cuda_solver* h, int32_t n, const fl
 int32_t insem_cuda_solver_n_columns(const insem_cuda_solver* h);
 /* Kernel launches of one captured step (the step graph's kernel nodes). */
 int32_t insem_cuda_solver_kernels_per_step(insem_cuda_solver* h);
+/* Elements per tile (one CTA) of the tiled path.  A solver takes
+ * options.tile_elements when > 0, else the entry set here for its domain's
+ * class (ngll, dominant geometry kind, medium, azimuthal order), else an
+ * occupancy-based default.  The autotuner (insem_b200.autotune) times
+ * candidates and sets the entries; tile_elements <= 0 clears one.  Applies to
+ * solvers created afterwards; process-wide. */
+int insem_cuda_set_tile_elements(int32_t ngll, int32_t kind, int32_t medium, int32_t azimuthal_order,
+                                 int32_t tile_elements);
+/* The choice a new solver would make for that class (ncomp: field components). */
+int32_t insem_cuda_tile_elements(int32_t ngll, int32_t kind, int32_t medium, int32_t azimuthal_order, int32_t ncomp);
+/* Elements per tile a solver's domain was built with (0 on the two-pass path). */
+int32_t insem_cuda_solver_tile_elements(const insem_cuda_solver* h, int32_t domain);
 /* Points of a domain finished inside their tile's kernel and by the halo
  * kernel (the roofline's split of the step's bytes). */
 int insem_cuda_solver_point_classes(const insem_cuda_solver* h, int32_t domain, int32_t* n_tile_points,

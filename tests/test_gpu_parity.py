@@ -164,3 +164,40 @@ def test_tiled_matches_plain_multi_tile(pkg, nx):
         if ep.size:
             assert np.array_equal(et[:, 0], ep[:, 0])
             assert np.abs(et[:, 1:] - ep[:, 1:]).max() <= 1e-9 * np.abs(ep[:, 1:]).max()
+
+
+@pytest.mark.parametrize("te", [3, 11, 64])
+@pytest.mark.parametrize("case", ["lay", "bh1"])
+def test_tile_size_does_not_change_results(pkg, case, te):
+    """Any elements-per-tile (CTA size) gives the reference's bits."""
+    z = golden(case)
+    prob, s = run_case(pkg, z, tile_elements=te)
+    with s:
+        for name, q in prob.trace_list():
+            assert np.array_equal(s.trace(name, q), z[f"run.trace.{name}.{q}"]), (case, te, name, q)
+        for di in range(len(prob.domains)):
+            u, v, a = s.state(prob.media[di])
+            assert np.array_equal(u, z[f"run.d{di}.u"].astype(np.float64).reshape(u.shape))
+
+
+def test_autotuner_registers_a_measured_choice(pkg):
+    from insem_b200 import autotune
+
+    prob = pkg.ProblemData.from_npz(golden("bh0"))
+    keys = autotune.classes_of(prob)
+    try:
+        table = autotune.tune([prob], steps=5)
+        assert set(table) == set(keys)
+        for k, v in table.items():
+            assert v["te"] in v["timings"] and autotune.current(k) == v["te"]
+        with pkg.Solver(prob) as s:
+            assert [s_te for s_te in (N_te(s, i) for i in range(len(prob.domains)))] == [table[k]["te"] for k in keys]
+    finally:
+        for k in keys:
+            autotune.register(k, 0)
+
+
+def N_te(s, domain):
+    from insem_b200 import native as N
+
+    return int(N.lib().insem_cuda_solver_tile_elements(s._h, domain))
