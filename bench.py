@@ -412,6 +412,32 @@ def bench_config4(args, world, rank, device, pg) -> dict:
     return line
 
 
+def bench_serving(args, device) -> dict:
+    """The serving stream through the continuous-batching server, and its first
+    part through the plain path (one solve at a time): same requests."""
+    import __graft_entry__ as entry
+
+    entry.load_package()
+    from insem_b200 import serving as S
+
+    stream = S.request_stream(rate=args.serve_rate, window=args.serve_window, time_scale=args.serve_scale)
+    t0 = time.perf_counter()
+    batched = S.summarize(S.Server(device=device, chunk_steps=args.serve_chunk).run(stream, keep_traces=False))
+    wall_b = time.perf_counter() - t0
+    sub = stream[: max(1, int(len(stream) * args.serve_plain_fraction))]
+    t0 = time.perf_counter()
+    plain = S.summarize(S.serve_plain(sub, device=device))
+    wall_p = time.perf_counter() - t0
+    out = {"workload": f"Poisson {args.serve_rate:g}/s over {args.serve_window:g} s: 40 % Cartesian (2k-200k "
+                       f"elements, order 3-8), 35 % monopole and 25 % dipole boreholes from the batched set; "
+                       f"simulated durations U(2, 8) ms x {args.serve_scale:g}",
+           "batched": batched, "plain": plain, "plain_requests": len(sub),
+           "wall_seconds": {"batched": round(wall_b, 1), "plain": round(wall_p, 1)}}
+    if batched.get("value") and plain.get("value"):
+        out["batched_over_plain"] = batched["value"] / plain["value"]
+    return out
+
+
 def run_ours(args, world, rank, local, pg):
     import torch
 
@@ -432,6 +458,8 @@ def run_ours(args, world, rank, local, pg):
         }
     else:
         line = bench_config4(args, world, rank, device, pg)
+        if not args.no_serving:
+            line["serving"] = bench_serving(args, device)
         if not args.no_config3:
             r = bench_config3(args, world, rank, device, pg, headline=False)
             line["plain_config3"] = {k: r[k] for k in ("value", "ms_per_step", "steps", "workload", "points",
@@ -465,6 +493,13 @@ def main():
     ap.add_argument("--config3-steps", type=int, default=200, help="steps of the config3 sub-run")
     ap.add_argument("--no-config3", action="store_true", help="skip the config3 sub-run")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload: keep the default tile sizes")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
+    ap.add_argument("--serve-rate", type=float, default=50.0, help="serving: mean arrivals per second")
+    ap.add_argument("--serve-window", type=float, default=10.0, help="serving: seconds of arrivals")
+    ap.add_argument("--serve-scale", type=float, default=0.01, help="serving: factor on the simulated durations")
+    ap.add_argument("--serve-chunk", type=int, default=32, help="serving: batched steps between admissions")
+    ap.add_argument("--serve-plain-fraction", type=float, default=0.25,
+                    help="serving: share of the stream (from its start) also served by the plain path")
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the streamed end-to-end run")

@@ -110,10 +110,12 @@ class Batch:
         return [m for m in self.members if m is not None and m.step < m.n_steps]
 
     def advance_streamed(self, n_steps: int, amplitudes, rows_out=None) -> int:
-        """Up to n_steps batched steps (stopping at the next completion) with
-        per-step host I/O: ``amplitudes`` [n_steps, amp_cols] float32 in,
-        ``rows_out`` [n_steps, row_cols] float64 out (numpy arrays or pinned
-        torch tensors).  Returns the steps done."""
+        """n_steps batched steps (fewer if every member ends sooner) with
+        per-step host I/O: ``amplitudes`` [n_steps, amp_cols] float32 in (None:
+        the members' own source time functions), ``rows_out`` [n_steps,
+        row_cols] float64 out (numpy arrays or pinned torch tensors).  A member
+        with r steps left has valid rows for its first r steps.  Returns the
+        steps done."""
         def ptr(x, ctype):
             if x is None:
                 return None
@@ -140,6 +142,11 @@ class Batch:
     @property
     def steps_to_next_completion(self) -> int:
         return int(N.lib().insem_cuda_batch_steps_to_next_completion(self._h))
+
+    @property
+    def steps_to_completion(self) -> int:
+        """Steps until every member is complete."""
+        return int(N.lib().insem_cuda_batch_steps_to_completion(self._h))
 
     @property
     def last_advance_ms(self) -> float:

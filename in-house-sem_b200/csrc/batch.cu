@@ -420,68 +420,82 @@ void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
   }
 }
 
+int32_t Batch::max_remaining() const {
+  int32_t k = 0;
+  for (const auto& m : members)
+    if (m) k = std::max(k, m->s->remaining());
+  return k;
+}
+
+// After k batched steps: each running solve did min(k, its remaining) steps
+// and idled after its last one.
+void Batch::credit(int32_t k) {
+  std::vector<Solver*> done;
+  for (std::size_t i = 0; i < members.size(); ++i) {
+    if (!members[i] || !prepared[i] || members[i]->s->remaining() <= 0) continue;
+    Solver& s = *members[i]->s;
+    const int32_t d = std::min(k, s.remaining());
+    s.batch_advanced(d);
+    point_updates += member_points[i] * d;
+    if (s.remaining() == 0) {
+      dirty = true;
+      done.push_back(&s);
+    }
+  }
+  INSEM_REQUIRE(!*herr, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
+  if (opts.check_finite)
+    for (Solver* s : done) s->check_fields();
+}
+
+void Batch::finish_steps() {
+  batch_error_kernel<<<ceil_div(std::max(n_states, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, derr.get());
+  CUDA_LAUNCH_CHECK();
+  CUDA_CHECK(cudaMemcpyAsync(herr, derr.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
+  CUDA_CHECK(cudaStreamSynchronize(stream));
+}
+
 void Batch::advance(int32_t n) {
   DeviceGuard dg(opts.device);
   INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
-  double total_ms = 0.0;
   point_updates = 0;
-  while (n > 0) {
-    const int32_t next = steps_to_next_completion();
-    if (next == 0) break;
-    if (dirty) rebuild();
-    const int32_t k = std::min(n, next);
-    CUDA_CHECK(cudaMemsetAsync(derr.get(), 0, sizeof(int32_t), stream));
-    CUDA_CHECK(cudaEventRecord(ev0, stream));
-    for (int32_t j = 0; j < k; ++j) {
-      if (graph) CUDA_CHECK(cudaGraphLaunch(graph, stream));
-      else enqueue();
-    }
-    CUDA_CHECK(cudaEventRecord(ev1, stream));
-    batch_error_kernel<<<ceil_div(std::max(n_states, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, derr.get());
-    CUDA_LAUNCH_CHECK();
-    CUDA_CHECK(cudaMemcpyAsync(herr, derr.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-    CUDA_CHECK(cudaStreamSynchronize(stream));
-    float ms = 0.0f;
-    CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
-    total_ms += ms;
-    std::vector<Solver*> done;
-    for (std::size_t i = 0; i < members.size(); ++i) {
-      if (!members[i] || !prepared[i] || members[i]->s->remaining() <= 0) continue;
-      Solver& s = *members[i]->s;
-      s.batch_advanced(k);
-      point_updates += member_points[i] * k;
-      if (s.remaining() == 0) {
-        dirty = true;
-        done.push_back(&s);
-      }
-    }
-    n -= k;
-    INSEM_REQUIRE(!*herr, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
-    if (opts.check_finite)
-      for (Solver* s : done) s->check_fields();
+  last_ms = 0.0;
+  const int32_t k = std::min(n, max_remaining());
+  if (k == 0) return;
+  if (dirty) rebuild();
+  CUDA_CHECK(cudaMemsetAsync(derr.get(), 0, sizeof(int32_t), stream));
+  CUDA_CHECK(cudaEventRecord(ev0, stream));
+  for (int32_t j = 0; j < k; ++j) {
+    if (graph) CUDA_CHECK(cudaGraphLaunch(graph, stream));
+    else enqueue();
   }
-  last_ms = total_ms;
+  CUDA_CHECK(cudaEventRecord(ev1, stream));
+  finish_steps();
+  float ms = 0.0f;
+  CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
+  last_ms = ms;
+  credit(k);
 }
 
 void Batch::stream_layout(int32_t* a, int32_t* r) {
   DeviceGuard dg(opts.device);
-  if (dirty && steps_to_next_completion() > 0) rebuild();
-  if (a) *a = steps_to_next_completion() > 0 ? amp_cols : 0;
-  if (r) *r = steps_to_next_completion() > 0 ? row_cols : 0;
+  const bool running = max_remaining() > 0;
+  if (dirty && running) rebuild();
+  if (a) *a = running ? amp_cols : 0;
+  if (r) *r = running ? row_cols : 0;
 }
 
 int32_t Batch::advance_streamed(int32_t n, const float* amp_in, double* rows_out) {
   DeviceGuard dg(opts.device);
   INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
-  const int32_t next = steps_to_next_completion();
-  if (next == 0 || n == 0) return 0;
+  point_updates = 0;
+  last_ms = 0.0;
+  const int32_t k = std::min(n, max_remaining());
+  if (k == 0) return 0;
   if (dirty) rebuild();
-  INSEM_REQUIRE(amp_cols == 0 || amp_in, INSEM_CUDA_ERR_INVALID, "missing source amplitudes");
-  const int32_t k = std::min(n, next);
   CUDA_CHECK(cudaMemsetAsync(derr.get(), 0, sizeof(int32_t), stream));
   CUDA_CHECK(cudaEventRecord(ev0, stream));
   for (int32_t j = 0; j < k; ++j) {
-    if (amp_cols > 0) {
+    if (amp_cols > 0 && amp_in) {
       CUDA_CHECK(cudaMemcpyAsync(amp_stage.get(), amp_in + static_cast<std::size_t>(j) * amp_cols,
                                  amp_cols * sizeof(float), cudaMemcpyHostToDevice, stream));
       batch_amp_scatter_kernel<<<n_stream, 64, 0, stream>>>(dstream.get(), amp_stage.get());
@@ -497,35 +511,19 @@ int32_t Batch::advance_streamed(int32_t n, const float* amp_in, double* rows_out
     }
   }
   CUDA_CHECK(cudaEventRecord(ev1, stream));
-  batch_error_kernel<<<ceil_div(std::max(n_states, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, derr.get());
-  CUDA_LAUNCH_CHECK();
-  CUDA_CHECK(cudaMemcpyAsync(herr, derr.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-  CUDA_CHECK(cudaStreamSynchronize(stream));
+  finish_steps();
   float ms = 0.0f;
   CUDA_CHECK(cudaEventElapsedTime(&ms, ev0, ev1));
   last_ms = ms;
-  point_updates = 0;
-  std::vector<Solver*> done;
-  for (std::size_t i = 0; i < members.size(); ++i) {
-    if (!members[i] || !prepared[i] || members[i]->s->remaining() <= 0) continue;
-    Solver& s = *members[i]->s;
-    s.batch_advanced(k);
-    point_updates += member_points[i] * k;
-    if (s.remaining() == 0) {
-      dirty = true;
-      done.push_back(&s);
-    }
-  }
-  INSEM_REQUIRE(!*herr, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
-  if (opts.check_finite)
-    for (Solver* s : done) s->check_fields();
+  credit(k);
   return k;
 }
 
 void Batch::profile(int32_t n, double* tile_ms, double* step_ms) {
   DeviceGuard dg(opts.device);
   INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
-  const int32_t k = std::min(n, steps_to_next_completion());
+  point_updates = 0;
+  const int32_t k = std::min(n, max_remaining());
   double tt = 0.0, ts = 0.0;
   if (k > 0) {
     if (dirty) rebuild();
@@ -537,10 +535,7 @@ void Batch::profile(int32_t n, double* tile_ms, double* step_ms) {
       enqueue(ev[4 * j + 1], ev[4 * j + 2]);
       CUDA_CHECK(cudaEventRecord(ev[4 * j + 3], stream));
     }
-    batch_error_kernel<<<ceil_div(std::max(n_states, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, derr.get());
-    CUDA_LAUNCH_CHECK();
-    CUDA_CHECK(cudaMemcpyAsync(herr, derr.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream));
-    CUDA_CHECK(cudaStreamSynchronize(stream));
+    finish_steps();
     for (int32_t j = 0; j < k; ++j) {
       float a = 0.0f, b = 0.0f;
       CUDA_CHECK(cudaEventElapsedTime(&a, ev[4 * j + 1], ev[4 * j + 2]));
@@ -549,30 +544,13 @@ void Batch::profile(int32_t n, double* tile_ms, double* step_ms) {
       ts += b;
     }
     for (auto& e : ev) cudaEventDestroy(e);
-    std::vector<Solver*> done;
-    for (std::size_t i = 0; i < members.size(); ++i) {
-      if (!members[i] || !prepared[i] || members[i]->s->remaining() <= 0) continue;
-      members[i]->s->batch_advanced(k);
-      if (members[i]->s->remaining() == 0) {
-        dirty = true;
-        done.push_back(members[i]->s.get());
-      }
-    }
-    INSEM_REQUIRE(!*herr, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
-    if (opts.check_finite)
-      for (Solver* s : done) s->check_fields();
+    credit(k);
   }
   if (tile_ms) *tile_ms = tt;
   if (step_ms) *step_ms = ts;
 }
 
-void Batch::run() {
-  for (;;) {
-    const int32_t k = steps_to_next_completion();
-    if (k == 0) break;
-    advance(k);
-  }
-}
+void Batch::run() { advance(max_remaining()); }
 
 }  // namespace insem_b200
 
@@ -668,6 +646,7 @@ int32_t insem_cuda_batch_active(const insem_cuda_batch* h) { return h ? h->b->ac
 int32_t insem_cuda_batch_steps_to_next_completion(const insem_cuda_batch* h) {
   return h ? h->b->steps_to_next_completion() : 0;
 }
+int32_t insem_cuda_batch_steps_to_completion(const insem_cuda_batch* h) { return h ? h->b->max_remaining() : 0; }
 double insem_cuda_batch_last_advance_ms(const insem_cuda_batch* h) { return h ? h->b->last_ms : 0.0; }
 int64_t insem_cuda_batch_point_updates(const insem_cuda_batch* h) { return h ? h->b->point_updates : 0; }
 int32_t insem_cuda_batch_kernels_per_step(const insem_cuda_batch* h) { return h ? h->b->kernels_per_step : 0; }

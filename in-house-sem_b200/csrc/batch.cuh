@@ -13,9 +13,9 @@
 //   receivers (particle velocity, then recording) and energy of every solve
 // Each solve keeps its own device data, time step, parity and step count,
 // so its results are the ones it gets alone, bit for bit.  Solves that
-// reach their last step run it in final mode and leave the batch; the
-// segment tables are rebuilt and the graph re-captured when membership
-// changes.
+// reach their last step run it in final mode and idle (every batched kernel
+// skips them) until the tables are rebuilt without them: membership changes
+// re-capture the graph at the next advance.
 #pragma once
 
 #include <map>
@@ -70,11 +70,11 @@ class Batch {
   int32_t add(const insem_cuda_problem& p);
   // Takes ownership of an existing solve that no batch has stepped.
   int32_t adopt(insem_cuda_solver* h);
-  // n batched steps (solves with fewer steps left stop at their end).
+  // n batched steps; a solve with fewer steps left idles after its last one.
   void advance(int32_t n);
   // Steps until every solve is complete.
   void run();
-  // Up to n steps (stopping at the next completion) with per-step host I/O:
+  // n steps (fewer if every solve ends sooner) with per-step host I/O:
   // amp_in[step][amp_cols] are the active solves' source amplitudes (in index
   // order, each solve's sources in order), rows_out[step][row_cols] their
   // latest sample rows.  Returns the steps done.
@@ -90,6 +90,7 @@ class Batch {
   int32_t size() const { return static_cast<int32_t>(members.size()); }
   int32_t active() const;
   int32_t steps_to_next_completion() const;
+  int32_t max_remaining() const;  // steps until every member is complete
 
   insem_cuda_options opts{};
   double last_ms = 0.0;           // device time of the last advance()
@@ -98,6 +99,8 @@ class Batch {
 
  private:
   void rebuild();
+  void finish_steps();       // error flags of the steps just enqueued; waits for them
+  void credit(int32_t k);    // host bookkeeping after k batched steps
   void enqueue(cudaEvent_t tiles_begin = nullptr, cudaEvent_t tiles_end = nullptr);
 
   struct DevClass {

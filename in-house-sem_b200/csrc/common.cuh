@@ -15,6 +15,8 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
+#include <set>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -77,6 +79,45 @@ int guarded(Fn&& fn) {
 }
 
 // ------------------------------------------------------------ device memory
+// Device memory comes from the current device's default stream-ordered pool,
+// in the legacy stream's order, and freed memory stays in the pool: freeing
+// does not wait for the whole device (as cudaFree does) and does not hand
+// memory back to the system, so solves can come and go while others run.
+// An owner frees memory only after its own stream has finished with it.
+inline void keep_pool_memory(int device) {
+  static std::mutex mu;
+  static std::set<int> done;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(device)) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  done.insert(device);
+}
+
+// Allocates `bytes` on the current device; usable on every stream on return.
+inline void* device_alloc(std::size_t bytes) {
+  int device = 0;
+  CUDA_CHECK(cudaGetDevice(&device));
+  keep_pool_memory(device);
+  void* p = nullptr;
+  const cudaError_t e = cudaMallocAsync(&p, bytes, nullptr);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(INSEM_CUDA_ERR_NOMEM, "device allocation of " + std::to_string(bytes) +
+                                          " bytes failed: " + cudaGetErrorString(e));
+  }
+  CUDA_CHECK(cudaStreamSynchronize(nullptr));
+  return p;
+}
+
+// Returns memory to the pool (the current device must be the one it came from).
+inline void device_free(void* p) {
+  if (p) cudaFreeAsync(p, nullptr);
+}
+
 // Owning device buffer.  Allocation failures report INSEM_CUDA_ERR_NOMEM.
 template <class T>
 class DeviceBuffer {
@@ -100,18 +141,17 @@ class DeviceBuffer {
   void resize(std::size_t n) {
     release();
     if (n == 0) return;
-    cudaError_t e = cudaMalloc(&p_, n * sizeof(T));
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      p_ = nullptr;
-      throw Error(INSEM_CUDA_ERR_NOMEM, "cudaMalloc of " + std::to_string(n * sizeof(T)) +
-                                            " bytes failed: " + cudaGetErrorString(e));
-    }
+    p_ = static_cast<T*>(device_alloc(n * sizeof(T)));
     n_ = n;
   }
   void upload(const T* host, std::size_t n) {
     resize(n);
-    if (n) CUDA_CHECK(cudaMemcpy(p_, host, n * sizeof(T), cudaMemcpyHostToDevice));
+    if (n) {
+      CUDA_CHECK(cudaMemcpy(p_, host, n * sizeof(T), cudaMemcpyHostToDevice));
+      // a copy from pageable memory may return before its DMA has landed;
+      // consumers run on other (non-blocking) streams
+      CUDA_CHECK(cudaStreamSynchronize(nullptr));
+    }
   }
   void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
   void zero(cudaStream_t s = nullptr) {
@@ -129,7 +169,7 @@ class DeviceBuffer {
 
  private:
   void release() {
-    if (p_) cudaFree(p_);
+    device_free(p_);
     p_ = nullptr;
     n_ = 0;
   }

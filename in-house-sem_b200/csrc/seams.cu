@@ -106,6 +106,16 @@ extern "C" {
 const char* insem_cuda_last_error(void) { return last_error(); }
 const char* insem_cuda_version(void) { return "insem-b200 0.1.0"; }
 
+int insem_cuda_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes) {
+  return guarded([&] {
+    DeviceGuard dg(device);
+    std::size_t f = 0, t = 0;
+    CUDA_CHECK(cudaMemGetInfo(&f, &t));
+    if (free_bytes) *free_bytes = static_cast<int64_t>(f);
+    if (total_bytes) *total_bytes = static_cast<int64_t>(t);
+  });
+}
+
 int insem_cuda_block_create(const insem_cuda_basis* basis, const insem_cuda_block* block, int32_t medium,
                             int32_t device, insem_cuda_block_h** out) {
   return guarded([&] {

@@ -20,6 +20,8 @@
 
 namespace insem_b200 {
 
+int32_t* pinned_modes();
+
 void DeviceDomainData::upload(const insem_cuda_domain& d, const insem_cuda_basis& basis) {
   medium = d.medium;
   INSEM_REQUIRE(medium == INSEM_ACOUSTIC || medium == INSEM_ELASTIC, INSEM_CUDA_ERR_INVALID, "unknown medium");
@@ -123,7 +125,7 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
   build_coupling(p.coupling);
   build_sources(p);
   build_receivers(p);
-  CUDA_CHECK(cudaMalloc(&st, sizeof(StepState)));
+  st = static_cast<StepState*>(device_alloc(sizeof(StepState)));
   CUDA_CHECK(cudaMemset(st, 0, sizeof(StepState)));
   partial.resize(static_cast<std::size_t>(kReduceBlocks) * 4);
   const int32_t n_energy = energy_every > 0 ? n_steps / energy_every + 1 : 0;
@@ -139,17 +141,19 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
   if (setup_only || opts.path == 1)
     for (auto& d : domains) d.alloc_fields();
   if (!setup_only && opts.path != 1) build_tiled(p);
+  // uploads and zeroing ran on the legacy stream and this solver's stream;
+  // other streams (other solvers, batches) are not waited for
   CUDA_CHECK(cudaStreamSynchronize(nullptr));
-  CUDA_CHECK(cudaDeviceSynchronize());
+  CUDA_CHECK(cudaStreamSynchronize(stream));
 }
 
 Solver::~Solver() {
   DeviceGuard dg(device);
+  if (stream) cudaStreamSynchronize(stream);  // buffers go back to the pool below
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   for (auto& g : tgraph)
     if (g) cudaGraphExecDestroy(g);
-  if (mode_host) cudaFreeHost(mode_host);
-  if (st) cudaFree(st);
+  device_free(st);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (stream) cudaStreamDestroy(stream);
@@ -402,65 +406,86 @@ double Solver::reduce_partials() {
 double Solver::stable_dt() {
   DeviceGuard dg(device);
   for (auto& d : domains) d.alloc_fields();
-  double lambda = 0.0;
   std::mt19937 rng(12345);
   std::uniform_real_distribution<double> dist(-1.0, 1.0);
+  DeviceBuffer<double> pw(kPwCount);
+  pw.zero(stream);
+  auto reduce_into = [&](int slot, double sign) {
+    sum_partials_kernel<<<1, kReduceBlocks, 0, stream>>>(partial.get(), kReduceBlocks, sign, pw.get(), slot);
+    CUDA_LAUNCH_CHECK();
+  };
   for (auto& d : domains) {
     const int64_t n = static_cast<int64_t>(d.ncomp) * d.ng;
     std::vector<float> x(n);
     for (auto& v : x) v = static_cast<float>(dist(rng));
-    DeviceBuffer<float> dx;
-    dx.upload(x);
+    DeviceBuffer<float> dx(n);
+    CUDA_CHECK(cudaMemcpyAsync(dx.get(), x.data(), n * sizeof(float), cudaMemcpyHostToDevice, stream));
+    CUDA_CHECK(cudaMemsetAsync(pw.get() + kPwDone, 0, sizeof(double), stream));
     for (int it = 0; it < 100; ++it) {
       zero_constrained(d, dx.get());
       internal_forces(d, dx.get(), d.f.get());
       dot_partial_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(dx.get(), d.f.get(), n, st, 0, 1,
                                                                        partial.get());
       CUDA_LAUNCH_CHECK();
-      const double xkx = -reduce_partials();
+      reduce_into(kPwA, -1.0);  // x.Kx = -(x . f_int)
       mass_norm_partial_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(dx.get(), d.mass.get(), d.ng,
                                                                              d.ncomp, partial.get());
       CUDA_LAUNCH_CHECK();
-      const double xmx = reduce_partials();
-      if (xmx > 0.0) lambda = std::max(lambda, xkx / xmx);
+      reduce_into(kPwB, 1.0);
       power_update_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(d.f.get(), d.inv_mass.get(), dx.get(),
                                                                         d.ng, d.ncomp, partial.get());
       CUDA_LAUNCH_CHECK();
-      const double norm = reduce_partials();
-      if (norm == 0.0) break;
-      scale_kernel<<<grid_for(n), 256, 0, stream>>>(dx.get(), dx.get(), n, 1.0 / std::sqrt(norm));
+      reduce_into(kPwNorm, 1.0);
+      power_step_kernel<<<1, 1, 0, stream>>>(pw.get());
+      CUDA_LAUNCH_CHECK();
+      scale_dev_kernel<<<grid_for(n), 256, 0, stream>>>(dx.get(), dx.get(), n, pw.get());
       CUDA_LAUNCH_CHECK();
     }
     d.f.zero(stream);
+    // dx is released below: its last kernels must have run
+    CUDA_CHECK(cudaStreamSynchronize(stream));
   }
-  if (n_cpl > 0) lambda = std::max(lambda, coupled_lambda_max(rng));
+  if (n_cpl > 0) coupled_lambda_max(rng, pw.get());
+  double h[kPwCount];
+  CUDA_CHECK(cudaMemcpyAsync(h, pw.get(), sizeof(h), cudaMemcpyDeviceToHost, stream));
   CUDA_CHECK(cudaStreamSynchronize(stream));
+  double lambda = h[kPwLambda];
+  if (n_cpl > 0) lambda = std::max(lambda, h[kPwCoupled]);
   INSEM_REQUIRE(lambda > 0.0, INSEM_CUDA_ERR_INVALID, "could not estimate the stable time step (empty or rigid model?)");
   return 2.0 / std::sqrt(lambda);
 }
 
 // coupled_lambda_max (solver.cpp:621-667): growth of the mass norm under the
-// coupled operator, 120 iterations, sqrt(ny / nx) from iteration 60 on.
-double Solver::coupled_lambda_max(std::mt19937& rng) {
+// coupled operator, 120 iterations, sqrt(ny / nx) from iteration 60 on; the
+// result lands in pw[kPwCoupled].
+void Solver::coupled_lambda_max(std::mt19937& rng, double* pw) {
   DeviceDomainData& sd = domains[solid];
   DeviceDomainData& fd = domains[fluid];
   std::uniform_real_distribution<double> dist(-1.0, 1.0);
+  std::vector<std::vector<float>> x0(2);
+  int q = 0;
   for (DeviceDomainData* d : {&sd, &fd}) {
-    std::vector<float> x(static_cast<std::size_t>(d->ncomp) * d->ng);
+    auto& x = x0[q++];
+    x.resize(static_cast<std::size_t>(d->ncomp) * d->ng);
     for (auto& v : x) v = static_cast<float>(dist(rng));
-    CUDA_CHECK(cudaMemcpy(d->u.get(), x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_CHECK(cudaMemcpyAsync(d->u.get(), x.data(), x.size() * sizeof(float), cudaMemcpyHostToDevice, stream));
   }
-  auto mass_norm2 = [&](DeviceDomainData& d, const float* x) {
+  CUDA_CHECK(cudaMemsetAsync(pw + kPwDone, 0, sizeof(double), stream));
+  CUDA_CHECK(cudaMemsetAsync(pw + kPwCoupled, 0, sizeof(double), stream));
+  auto mass_norm = [&](DeviceDomainData& d, const float* x, int slot) {
     mass_norm_partial_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(x, d.mass.get(), d.ng, d.ncomp,
                                                                            partial.get());
     CUDA_LAUNCH_CHECK();
-    return reduce_partials();
+    sum_partials_kernel<<<1, kReduceBlocks, 0, stream>>>(partial.get(), kReduceBlocks, 1.0, pw, slot);
+    CUDA_LAUNCH_CHECK();
   };
-  double lambda = 0.0;
   for (int it = 0; it < 120; ++it) {
     zero_constrained(sd, sd.u.get());
     zero_constrained(fd, fd.u.get());
-    const double nx = mass_norm2(sd, sd.u.get()) + mass_norm2(fd, fd.u.get());
+    mass_norm(sd, sd.u.get(), kPwA);
+    mass_norm(fd, fd.u.get(), kPwB);
+    sum_ab_kernel<<<1, 1, 0, stream>>>(pw, kPwNx);
+    CUDA_LAUNCH_CHECK();
     for (int di : {solid, fluid}) {
       DeviceDomainData& d = domains[di];
       internal_forces(d, d.u.get(), d.f.get());
@@ -470,13 +495,15 @@ double Solver::coupled_lambda_max(std::mt19937& rng) {
       CUDA_LAUNCH_CHECK();
       zero_constrained(d, d.a.get());
     }
-    const double ny = mass_norm2(sd, sd.a.get()) + mass_norm2(fd, fd.a.get());
-    if (nx <= 0.0 || ny <= 0.0) break;
-    if (it >= 60) lambda = std::max(lambda, std::sqrt(ny / nx));
-    const double scale = -1.0 / std::sqrt(ny);
+    mass_norm(sd, sd.a.get(), kPwA);
+    mass_norm(fd, fd.a.get(), kPwB);
+    sum_ab_kernel<<<1, 1, 0, stream>>>(pw, kPwNy);
+    CUDA_LAUNCH_CHECK();
+    coupled_step_kernel<<<1, 1, 0, stream>>>(pw, it);
+    CUDA_LAUNCH_CHECK();
     for (DeviceDomainData* d : {&sd, &fd}) {
       const int64_t n = static_cast<int64_t>(d->ncomp) * d->ng;
-      scale_kernel<<<grid_for(n), 256, 0, stream>>>(d->a.get(), d->u.get(), n, scale);
+      scale_dev_kernel<<<grid_for(n), 256, 0, stream>>>(d->a.get(), d->u.get(), n, pw);
       CUDA_LAUNCH_CHECK();
     }
   }
@@ -485,7 +512,7 @@ double Solver::coupled_lambda_max(std::mt19937& rng) {
     d->a.zero(stream);
     d->f.zero(stream);
   }
-  return lambda;
+  CUDA_CHECK(cudaStreamSynchronize(stream));  // the host start vectors are read until here
 }
 
 // Kernels of the whole acceleration solve, elastic first (solver.cpp:674).
@@ -805,10 +832,7 @@ void Solver::build_tiled(const insem_cuda_problem& p) {
   }
   epart.resize(2 * static_cast<std::size_t>(std::max(base, 1)));
   epart.zero();
-  CUDA_CHECK(cudaMallocHost(&mode_host, 4 * sizeof(int32_t)));
-  mode_host[0] = kModeNormal;
-  mode_host[1] = kModeFinal;
-  mode_host[2] = kModeInit;
+  mode_host = pinned_modes();
   tiled = true;
 }
 
@@ -817,6 +841,21 @@ AllFields Solver::tiled_fields(int par) {
   for (std::size_t i = 0; i < tdom.size() && i < 2; ++i)
     f.d[i] = {tdom[i].u_cur(par), tdom[i].vn.get(), tdom[i].a.get(), tdom[i].ng};
   return f;
+}
+
+// Pinned {normal, final, init} shared by every solver for the whole process
+// (a per-solver pinned buffer would cost a device-wide wait when freed).
+int32_t* pinned_modes() {
+  static std::once_flag once;
+  static int32_t* modes = nullptr;
+  std::call_once(once, [] {
+    CUDA_CHECK(cudaMallocHost(&modes, 4 * sizeof(int32_t)));
+    modes[0] = kModeNormal;
+    modes[1] = kModeFinal;
+    modes[2] = kModeInit;
+    modes[3] = kModeIdle;
+  });
+  return modes;
 }
 
 void Solver::set_mode(int mode) {

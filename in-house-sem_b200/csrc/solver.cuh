@@ -93,7 +93,7 @@ class Solver {
   double reduce_partials();
   void zero_constrained(DeviceDomainData& d, float* x);
   void coupling_forces(int di);
-  double coupled_lambda_max(std::mt19937& rng);
+  void coupled_lambda_max(std::mt19937& rng, double* pw);
 
   DeviceBasis basis;
   int solid = -1, fluid = -1;

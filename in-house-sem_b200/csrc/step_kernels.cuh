@@ -379,6 +379,85 @@ static __global__ void scale_kernel(const float* __restrict__ src, float* __rest
     x[i] = static_cast<float>(dmul(static_cast<double>(src[i]), scale));
 }
 
+// Power-iteration scalars kept on the device, so an iteration needs no host
+// round trip: the partial sums, their reductions and the scalar logic of
+// estimate_stable_dt / coupled_lambda_max (solver.cpp:583-667) all run in
+// stream order; the host reads the result once.
+enum PowerSlot : int {
+  kPwLambda = 0,   // running max of the Rayleigh quotients (uncoupled domains)
+  kPwA = 1,        // reduction results
+  kPwB = 2,
+  kPwNorm = 3,
+  kPwDone = 4,     // the loop has stopped (the reference's break)
+  kPwScale = 5,    // factor of the next scaling
+  kPwNx = 6,
+  kPwNy = 7,
+  kPwCoupled = 8,  // running max of sqrt(ny / nx) (coupled operator)
+  kPwCount = 9
+};
+
+// pw[slot] = sign x (sum of partial[0..n) in index order, as the host loop
+// adds them).  One CTA of kReduceBlocks threads stages the partials in shared
+// memory with parallel loads; thread 0 then adds them in order.
+static __global__ void __launch_bounds__(kReduceBlocks) sum_partials_kernel(const double* __restrict__ partial, int n,
+                                                                          double sign, double* pw, int slot) {
+  __shared__ double sh[kReduceBlocks];
+  for (int i = threadIdx.x; i < n && i < kReduceBlocks; i += blockDim.x) sh[i] = partial[i];
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 0; i < n && i < kReduceBlocks; ++i) s = dadd(s, sh[i]);
+  pw[slot] = sign < 0.0 ? -s : s;
+}
+
+// pw[dst] = pw[kPwA] + pw[kPwB]
+static __global__ void sum_ab_kernel(double* pw, int dst) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) pw[dst] = dadd(pw[kPwA], pw[kPwB]);
+}
+
+// One uncoupled power iteration's scalars (solver.cpp:597-612): lambda from
+// x.Kx / x.Mx, then stop on a zero norm or set the scale 1 / sqrt(norm).
+static __global__ void power_step_kernel(double* pw) {
+  if (blockIdx.x != 0 || threadIdx.x != 0 || pw[kPwDone] != 0.0) return;
+  const double xmx = pw[kPwB];
+  if (xmx > 0.0) {
+    const double q = pw[kPwA] / xmx;
+    if (pw[kPwLambda] < q) pw[kPwLambda] = q;
+  }
+  const double norm = pw[kPwNorm];
+  if (norm == 0.0) {
+    pw[kPwDone] = 1.0;
+    return;
+  }
+  pw[kPwScale] = 1.0 / sqrt(norm);
+}
+
+// One coupled iteration's scalars (solver.cpp:641-662): stop on a zero norm,
+// sqrt(ny / nx) from iteration 60 on, scale -1 / sqrt(ny).
+static __global__ void coupled_step_kernel(double* pw, int it) {
+  if (blockIdx.x != 0 || threadIdx.x != 0 || pw[kPwDone] != 0.0) return;
+  const double nx = pw[kPwNx], ny = pw[kPwNy];
+  if (nx <= 0.0 || ny <= 0.0) {
+    pw[kPwDone] = 1.0;
+    return;
+  }
+  if (it >= 60) {
+    const double q = sqrt(ny / nx);
+    if (pw[kPwCoupled] < q) pw[kPwCoupled] = q;
+  }
+  pw[kPwScale] = -1.0 / sqrt(ny);
+}
+
+// x = (float)(src * pw[kPwScale]) unless the loop has stopped.
+static __global__ void scale_dev_kernel(const float* __restrict__ src, float* __restrict__ x, int64_t n,
+                                        const double* __restrict__ pw) {
+  if (pw[kPwDone] != 0.0) return;
+  const double scale = pw[kPwScale];
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    x[i] = static_cast<float>(dmul(static_cast<double>(src[i]), scale));
+}
+
 // Sets st->nonfinite if any entry of x is NaN or Inf.
 static __global__ void finite_check_kernel(const float* __restrict__ x, int64_t n, StepState* st) {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;

@@ -33,7 +33,8 @@ namespace insem_b200 {
 // GLL derivative matrix, GLJ derivative matrix and w_i w_j per ngll (2..9).
 static __constant__ float c_basis[8][3][81];
 
-enum StepMode : int32_t { kModeNormal = 0, kModeFinal = 1, kModeInit = 2 };
+// kModeIdle: a batched solve past its last step (the batch's kernels skip it).
+enum StepMode : int32_t { kModeNormal = 0, kModeFinal = 1, kModeInit = 2, kModeIdle = 3 };
 
 // Slot descriptor bits.
 constexpr uint32_t kSlotPointMask = 0xffffu;      // tile point index
@@ -564,7 +565,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ __align__(16) TileSeg s_seg;  // the item's segment, read by the body from shared memory
-  __shared__ int32_t s_item, s_segi, s_tile;
+  __shared__ int32_t s_item, s_segi, s_tile, s_idle;
   static_assert(sizeof(TileSeg) % 4 == 0, "TileSeg is copied as 32-bit words");
   if (threadIdx.x == 0) mbar_init(&bar, 1);
   __syncthreads();
@@ -587,12 +588,16 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
       for (int q = threadIdx.x; q < static_cast<int>(sizeof(TileSeg) / 4); q += blockDim.x) dst[q] = src[q];
     }
     __syncthreads();
-    if (threadIdx.x == 0 && s_seg.st->parity) {
-      const float* cur = s_seg.td.u_cur;
-      s_seg.td.u_cur = s_seg.td.u_nxt;
-      s_seg.td.u_nxt = const_cast<float*>(cur);
+    if (threadIdx.x == 0) {
+      s_idle = s_seg.st->mode == kModeIdle;
+      if (s_seg.st->parity) {
+        const float* cur = s_seg.td.u_cur;
+        s_seg.td.u_cur = s_seg.td.u_nxt;
+        s_seg.td.u_nxt = const_cast<float*>(cur);
+      }
     }
     __syncthreads();
+    if (s_idle) continue;  // a finished solve: no copies issued, the barrier phase is unchanged
     const int32_t local = s_tile;
     const bool ok = tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial,
                                                     s_seg.tile0 + local, L, smem_raw, &bar, phase);
@@ -843,6 +848,7 @@ static __global__ void __launch_bounds__(kHaloChunk) halo_batch_kernel(const Hal
                                                                          const int2* __restrict__ items) {
   const int2 it = items[blockIdx.x];
   const HaloSeg& sg = segs[it.x];
+  if (sg.st->mode == kModeIdle) return;
   const int par = sg.st->parity;
   TiledDev td = sg.td;
   if (par) {
@@ -870,6 +876,7 @@ static __global__ void __launch_bounds__(kConsChunk) constrained_batch_kernel(co
                                                                                const int2* __restrict__ items) {
   const int2 it = items[blockIdx.x];
   const ConsSeg& sg = segs[it.x];
+  if (sg.st->mode == kModeIdle) return;
   constrained_gather_body(sg.n, sg.row_of, sg.rows, sg.st->parity ? sg.u1 : sg.u0, sg.ng, sg.ncomp, sg.cval,
                           it.y * kConsChunk + static_cast<int32_t>(threadIdx.x));
 }
@@ -892,6 +899,7 @@ static __global__ void __launch_bounds__(kRecChunk) particle_velocity_batch_kern
                                                                                    const int2* __restrict__ items) {
   const int2 it = items[blockIdx.x];
   const RecSeg& sg = segs[it.x];
+  if (sg.st->mode == kModeIdle) return;
   particle_velocity_body(sg.rv, sg.st->parity ? sg.f1 : sg.f0, sg.acoustic_recv, sg.n_acoustic, sg.dt, 0,
                          it.y * kRecChunk + static_cast<int32_t>(threadIdx.x));
 }
@@ -900,6 +908,7 @@ static __global__ void __launch_bounds__(kRecChunk) record_batch_kernel(const Re
                                                                         const int2* __restrict__ items) {
   const int2 it = items[blockIdx.x];
   const RecSeg& sg = segs[it.x];
+  if (sg.st->mode == kModeIdle) return;
   record_body(sg.rv, sg.st->parity ? sg.f1 : sg.f0, sg.cols, sg.n_cols, sg.st->step, sg.record_every, sg.traces,
               sg.max_samples, it.y * kRecChunk + static_cast<int32_t>(threadIdx.x));
 }
@@ -917,20 +926,25 @@ struct EnergySeg {
 
 static __global__ void __launch_bounds__(kReduceThreads) energy_batch_kernel(const EnergySeg* __restrict__ segs) {
   const EnergySeg& sg = segs[blockIdx.x];
+  if (sg.st->mode == kModeIdle) return;
   tiled_energy_body(sg.epartial, sg.n_dom, sg.s0, sg.s1, sg.st, sg.energy_every, sg.dt, sg.energy, sg.max_samples);
 }
 
 // First kernel of a batched step: every solve's step counter, buffer parity
-// and mode (final on its last step), and the tile queues reset.
+// and mode (final on its last step, idle after it), and the tile queues reset.
 static __global__ void batch_begin_kernel(StepState* const* __restrict__ sts, int32_t n, int32_t* __restrict__ queues,
                                           int32_t n_queues) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n_queues) queues[i] = 0;
   if (i < n) {
     StepState* s = sts[i];
-    s->step += 1;
-    s->parity ^= 1;
-    s->mode = s->step == s->last_step ? kModeFinal : kModeNormal;
+    if (s->step >= s->last_step) {
+      s->mode = kModeIdle;
+    } else {
+      s->step += 1;
+      s->parity ^= 1;
+      s->mode = s->step == s->last_step ? kModeFinal : kModeNormal;
+    }
   }
 }
 

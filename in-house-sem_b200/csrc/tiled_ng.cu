@@ -1,7 +1,7 @@
 // Tile-kernel launchers and the constant-memory basis for one number of GLL
 // points, selected with -DINSEM_NG=<2..9> (one object per value).  Every
 // object has its own copy of c_basis; the host writes the entry of this
-// object's ngll through set_constant_basis_ng<N>.
+// object's ngll through set_constant_basis_ng<N>, once per device and part.
 #include "tiled_path.cuh"
 
 #ifndef INSEM_NG
@@ -15,15 +15,16 @@ namespace insem_b200 {
 
 void INSEM_CAT(launch_tiles_ng, INSEM_NG)(const TileLaunch& a) { launch_tiles_cfg<INSEM_NG>(a); }
 
+// Writes the given parts of this ngll's constant basis (a null part is left as it is).
 void INSEM_CAT(set_constant_basis_ng, INSEM_NG)(const float* D, const float* Dj, const float* w2) {
   constexpr int n = INSEM_NG * INSEM_NG;
-  float buf[3][81] = {};
-  for (int q = 0; q < n; ++q) {
-    buf[0][q] = D[q];
-    buf[1][q] = Dj ? Dj[q] : 0.0f;
-    buf[2][q] = w2[q];
+  const float* parts[3] = {D, Dj, w2};
+  for (int which = 0; which < 3; ++which) {
+    if (!parts[which]) continue;
+    float buf[81] = {};
+    for (int q = 0; q < n; ++q) buf[q] = parts[which][q];
+    CUDA_CHECK(cudaMemcpyToSymbol(c_basis, buf, sizeof(buf), sizeof(float) * 81 * (3 * (INSEM_NG - 2) + which)));
   }
-  CUDA_CHECK(cudaMemcpyToSymbol(c_basis, buf, sizeof(buf), sizeof(buf) * (INSEM_NG - 2)));
 }
 
 int INSEM_CAT(tile_elements_ng, INSEM_NG)() { return TileCfg<INSEM_NG>::TE; }

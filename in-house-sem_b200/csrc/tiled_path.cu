@@ -41,19 +41,55 @@ int tile_elements_ng7();
 int tile_elements_ng8();
 int tile_elements_ng9();
 
+namespace {
+// What each device's constant basis holds per ngll.  Solves of one ngll share
+// the bank: D and w2 are written by the first solve and must agree after; the
+// GLJ matrix is written by the first solve that has axial elements and never
+// cleared (a solve without it does not read it).  So a bank is written at most
+// once per part, never while kernels of that ngll that read the part run.
+struct BasisBank {
+  std::vector<float> D, Dj, w2;
+};
+std::mutex g_basis_mutex;
+std::map<std::pair<int, int>, BasisBank> g_basis;  // (device, ngll)
+
+void write_basis(int ngll, const float* D, const float* Dj, const float* w2) {
+  switch (ngll) {
+    case 2: set_constant_basis_ng2(D, Dj, w2); break;
+    case 3: set_constant_basis_ng3(D, Dj, w2); break;
+    case 4: set_constant_basis_ng4(D, Dj, w2); break;
+    case 5: set_constant_basis_ng5(D, Dj, w2); break;
+    case 6: set_constant_basis_ng6(D, Dj, w2); break;
+    case 7: set_constant_basis_ng7(D, Dj, w2); break;
+    case 8: set_constant_basis_ng8(D, Dj, w2); break;
+    case 9: set_constant_basis_ng9(D, Dj, w2); break;
+    default: check_ngll(ngll);
+  }
+}
+}  // namespace
+
 void set_constant_basis(int ngll, const std::vector<float>& D, const std::vector<float>& Dj,
                         const std::vector<float>& w2) {
-  const float* dj = Dj.empty() ? nullptr : Dj.data();
-  switch (ngll) {
-    case 2: set_constant_basis_ng2(D.data(), dj, w2.data()); break;
-    case 3: set_constant_basis_ng3(D.data(), dj, w2.data()); break;
-    case 4: set_constant_basis_ng4(D.data(), dj, w2.data()); break;
-    case 5: set_constant_basis_ng5(D.data(), dj, w2.data()); break;
-    case 6: set_constant_basis_ng6(D.data(), dj, w2.data()); break;
-    case 7: set_constant_basis_ng7(D.data(), dj, w2.data()); break;
-    case 8: set_constant_basis_ng8(D.data(), dj, w2.data()); break;
-    case 9: set_constant_basis_ng9(D.data(), dj, w2.data()); break;
-    default: check_ngll(ngll);
+  check_ngll(ngll);
+  int device = 0;
+  CUDA_CHECK(cudaGetDevice(&device));
+  std::lock_guard<std::mutex> lk(g_basis_mutex);
+  BasisBank& bank = g_basis[{device, ngll}];
+  if (bank.D.empty()) {
+    write_basis(ngll, D.data(), nullptr, w2.data());
+    bank.D = D;
+    bank.w2 = w2;
+  } else {
+    INSEM_REQUIRE(bank.D == D && bank.w2 == w2, INSEM_CUDA_ERR_INVALID,
+                  "solves of one ngll must share the GLL basis (D, w_i w_j)");
+  }
+  if (!Dj.empty()) {
+    if (bank.Dj.empty()) {
+      write_basis(ngll, nullptr, Dj.data(), nullptr);
+      bank.Dj = Dj;
+    } else {
+      INSEM_REQUIRE(bank.Dj == Dj, INSEM_CUDA_ERR_INVALID, "solves of one ngll must share the GLJ derivative matrix");
+    }
   }
 }
 

@@ -109,6 +109,7 @@ def lib() -> C.CDLL:
         sig = {
             "insem_cuda_last_error": (C.c_char_p, []),
             "insem_cuda_version": (C.c_char_p, []),
+            "insem_cuda_mem_info": (C.c_int, [C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
             "insem_cuda_block_create": (C.c_int, [C.POINTER(Basis), C.POINTER(Block), C.c_int32, C.c_int32, C.POINTER(vp)]),
             "insem_cuda_block_destroy": (None, [vp]),
             "insem_cuda_block_forces": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
@@ -156,6 +157,7 @@ def lib() -> C.CDLL:
             "insem_cuda_batch_size": (C.c_int32, [vp]),
             "insem_cuda_batch_active": (C.c_int32, [vp]),
             "insem_cuda_batch_steps_to_next_completion": (C.c_int32, [vp]),
+            "insem_cuda_batch_steps_to_completion": (C.c_int32, [vp]),
             "insem_cuda_batch_last_advance_ms": (C.c_double, [vp]),
             "insem_cuda_batch_point_updates": (C.c_int64, [vp]),
             "insem_cuda_batch_kernels_per_step": (C.c_int32, [vp]),

@@ -18,7 +18,7 @@
  *   insem_cuda_stable_dt   Solver::estimate_stable_dt + coupled_lambda_max
  *                          (cpp/src/solver/solver.cpp:583-667), FP64 reductions
  *   insem_cuda_batch_*     many independent solves advanced by shared launches
- *   insem_cuda_server_*    continuous-batching request loop
+ *                          (the serving loop admits and retires solves through it)
  *
  * Conventions follow the reference:
  *   - real_t is float: every field, metric and coefficient array is float;
@@ -62,6 +62,8 @@ extern "C" {
 const char* insem_cuda_last_error(void);
 /* Library version string. */
 const char* insem_cuda_version(void);
+/* Free and total device memory (bytes) of a device: the serving loop's HBM admission. */
+int insem_cuda_mem_info(int32_t device, int64_t* free_bytes, int64_t* total_bytes);
 
 /* ------------------------------------------------------------------- enums */
 enum insem_cuda_medium { INSEM_ACOUSTIC = 0, INSEM_ELASTIC = 1 }; /* description.hpp:17 */
@@ -325,7 +327,9 @@ void insem_cuda_batch_destroy(insem_cuda_batch* h);
 int insem_cuda_batch_add(insem_cuda_batch* h, const insem_cuda_problem* problem, int32_t* index);
 /* Takes ownership of a solver handle that has not been stepped by a batch. */
 int insem_cuda_batch_adopt(insem_cuda_batch* h, insem_cuda_solver* solver, int32_t* index);
-/* n batched steps; a solve with fewer steps left stops at its last step. */
+/* n batched steps (fewer if every member ends sooner); a member with fewer
+ * steps left runs its last step in final mode and then idles: the batch's
+ * kernels skip it until the next composition leaves it out. */
 int insem_cuda_batch_advance(insem_cuda_batch* h, int32_t n);
 /* Steps until every member is complete. */
 int insem_cuda_batch_run(insem_cuda_batch* h);
@@ -333,25 +337,29 @@ int insem_cuda_batch_run(insem_cuda_batch* h);
 int insem_cuda_batch_remove(insem_cuda_batch* h, int32_t index);
 /* Borrowed handle of member `index` (NULL and an error message if there is none). */
 insem_cuda_solver* insem_cuda_batch_member(insem_cuda_batch* h, int32_t index);
-/* Streamed batched steps (end-to-end serving form): up to n steps, stopping
- * at the next member completion; *n_done is the number done.  Per step it
- * takes amp_in[step][amp_cols], the source amplitudes of the active members
+/* Streamed batched steps (end-to-end serving form): n steps (fewer if every
+ * member ends sooner); *n_done is the number done.  A member with r < n steps
+ * left has valid rows for its first r steps.  Per step it takes
+ * amp_in[step][amp_cols], the source amplitudes of the members running at
+ * the call
  * (index order, each member's sources in order, FP32 as the reference casts
  * them), and writes rows_out[step][row_cols], each active member's latest
  * sample row (its columns as insem_cuda_solver_n_columns lays them out); one
- * host-to-device and one device-to-host copy per step.  rows_out may be NULL. */
+ * host-to-device and one device-to-host copy per step.  amp_in NULL: the
+ * solves' own source time functions (resident tables); rows_out may be NULL. */
 int insem_cuda_batch_advance_streamed(insem_cuda_batch* h, int32_t n, const float* amp_in, double* rows_out,
                                       int32_t* n_done);
 /* n steps with plain launches and CUDA events around each step's tile
- * launches (stops at the next completion): device ms of the tile launches
+ * launches (as insem_cuda_batch_advance): device ms of the tile launches
  * and of the whole steps. */
 int insem_cuda_batch_profile(insem_cuda_batch* h, int32_t n, double* tile_ms, double* step_ms);
-/* amp_cols and row_cols of the current composition (0 when nothing is running). */
+/* amp_cols and row_cols of the members running now (0 when none is). */
 int insem_cuda_batch_stream_layout(insem_cuda_batch* h, int32_t* amp_cols, int32_t* row_cols);
 int32_t insem_cuda_batch_size(const insem_cuda_batch* h);
 int32_t insem_cuda_batch_active(const insem_cuda_batch* h);
-/* Steps until the next member completes (0 when none is running). */
+/* Steps until the next member completes, and until all are (0 when none is running). */
 int32_t insem_cuda_batch_steps_to_next_completion(const insem_cuda_batch* h);
+int32_t insem_cuda_batch_steps_to_completion(const insem_cuda_batch* h);
 /* Device time of the last advance / run segment, ms; points x steps it did. */
 double insem_cuda_batch_last_advance_ms(const insem_cuda_batch* h);
 int64_t insem_cuda_batch_point_updates(const insem_cuda_batch* h);

@@ -1,0 +1,67 @@
+"""Serving on the GPU: requests that arrive while others run join the running
+batch; each request's streamed traces equal its solo run, bit for bit (the
+same result alone and in the mix)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_stream():
+    from insem_b200 import serving as S
+
+    stream = S.request_stream(rate=300.0, window=1.0, time_scale=0.004, max_requests=14)
+    for r in stream:
+        if r.kind.startswith("cartesian"):
+            r.spec["elements"] = min(r.spec["elements"], 5000.0)
+    return stream
+
+
+def _solo_traces(req):
+    from insem_b200 import Solver, cases as K, serving as S
+
+    model, arrays, _ = S.setup_request(req)
+    prob = K.build_from_arrays(model, arrays)
+    with Solver(prob) as s:
+        s.run()
+        return np.concatenate([s.trace_by_index(t) for t in range(len(prob.trace_list()))], axis=1)
+
+
+def test_served_results_equal_solo_runs(pkg):
+    from insem_b200 import serving as S
+
+    stream = _small_stream()
+    assert len({r.kind for r in stream}) >= 3
+    recs = S.Server(chunk_steps=7).run(stream)
+    summ = S.summarize(recs)
+    assert summ["completed"] == len(stream)
+    assert np.isfinite(summ["p99_ms_from_admission"]) and summ["value"] > 0
+    for r in stream:
+        rec = recs[r.rid]
+        solo = _solo_traces(r)
+        assert rec.traces.shape == solo.shape, (r.rid, r.kind)
+        assert np.array_equal(rec.traces, solo), (r.rid, r.kind)
+
+
+def test_small_budget_serialises_admission(pkg):
+    """With an HBM budget below two requests, each admission waits for the previous completion."""
+    from insem_b200 import serving as S
+
+    stream = _small_stream()[:5]
+    recs = S.Server(hbm_budget=1, chunk_steps=16).run(stream, keep_traces=False)
+    order = sorted(recs.values(), key=lambda r: r.admitted)
+    for a, b in zip(order, order[1:]):
+        assert b.admitted >= a.completed
+    assert all(np.isfinite(r.completed) for r in recs.values())
+
+
+def test_plain_server_runs_the_same_stream(pkg):
+    from insem_b200 import serving as S
+
+    stream = _small_stream()[:4]
+    recs = S.serve_plain(stream, keep_traces=True)
+    for r in stream:
+        assert np.array_equal(recs[r.rid].traces, _solo_traces(r))
