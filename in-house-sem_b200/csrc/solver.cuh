@@ -66,6 +66,9 @@ class Solver {
   void internal_forces(DeviceDomainData& d, const float* u_global, float* f_global);
   // Power iteration for lambda_max(M^-1 K) (solver.cpp:583-667); returns 2/sqrt(lambda).
   double stable_dt();
+  // f = -K u of domain di on the caller's device arrays, without allocating
+  // (the element-local forces use a fixed array, see noalloc.cu).
+  void internal_forces_noalloc(int32_t di, const float* u_global, float* f_global, cudaStream_t s);
 
   insem_cuda_options opts{};
   int device = 0;

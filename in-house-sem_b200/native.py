@@ -135,6 +135,7 @@ def lib() -> C.CDLL:
             "insem_cuda_solver_state": (C.c_int, [vp, C.c_int32, f64p, f64p, f64p]),
             "insem_cuda_solver_last_advance_ms": (C.c_double, [vp]),
             "insem_cuda_solver_internal_forces": (C.c_int, [vp, C.c_int32, f32p, f32p]),
+            "insem_cuda_solver_internal_forces_noalloc": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
             "insem_cuda_stable_dt": (C.c_int, [C.POINTER(Problem), C.c_int32, f64p]),
             "insem_cuda_solver_advance_streamed": (C.c_int, [vp, C.c_int32, f32p, f64p, i32p]),
             "insem_cuda_solver_n_columns": (C.c_int32, [vp]),

@@ -299,6 +299,25 @@ int insem_cuda_set_tile_elements(int32_t ngll, int32_t kind, int32_t medium, int
 int32_t insem_cuda_tile_elements(int32_t ngll, int32_t kind, int32_t medium, int32_t azimuthal_order, int32_t ncomp);
 /* Elements per tile a solver's domain was built with (0 on the two-pass path). */
 int32_t insem_cuda_solver_tile_elements(const insem_cuda_solver* h, int32_t domain);
+/* Internal forces f = -K u of one domain, like insem_cuda_solver_internal_forces,
+ * for callers that cannot have the library allocate device memory: u and f
+ * are device arrays the caller owns ([ncomp][n_global], the reference's
+ * numbering), the work is enqueued on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream) and the call returns without waiting for it.  No
+ * counterpart in the reference: it adds an allocation-free form of the
+ * internal_forces seam (solver.cpp:570-581).
+ *   - Nothing is allocated or freed: the element-local force vectors go to a
+ *     fixed 16 MiB device array inside the library (4,194,304 floats), which
+ *     every GPU that loads the library holds until the process exits.  A
+ *     domain needing more (ncomp x elements x ngll^2 floats) is rejected with
+ *     INSEM_CUDA_ERR_UNSUPPORTED before anything is enqueued.
+ *   - The first call on a device looks up the array's device address (once
+ *     per device); make that first call before any stream capture.
+ *   - All calls share the array: calls whose work overlaps on the GPU (other
+ *     streams, other threads, other handles) race on it.  Each call clears
+ *     the part it uses before use. */
+int insem_cuda_solver_internal_forces_noalloc(insem_cuda_solver* h, int32_t domain, const float* u, float* f,
+                                              void* stream);
 /* Points of a domain finished inside their tile's kernel and by the halo
  * kernel (the roofline's split of the step's bytes). */
 int insem_cuda_solver_point_classes(const insem_cuda_solver* h, int32_t domain, int32_t* n_tile_points,
