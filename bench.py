@@ -112,7 +112,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def dist_setup(n_gpus: int):
+def dist_setup(n_gpus: int, backend: str = "nccl"):
+    """Rank, world and process group from the torchrun environment (replicas:
+    no collective touches the data path; the group carries the barrier and
+    the max over ranks only).  backend "gloo" runs the same logic on CPU."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -123,28 +126,37 @@ def dist_setup(n_gpus: int):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
     return world, rank, local, pg
 
 
-def reduce_max(pg, value: float, device: int) -> float:
+def reduce_max(pg, value: float, device) -> float:
+    """Max of `value` over ranks (device None: a CPU tensor, for gloo)."""
     if pg is None:
         return value
     import torch
 
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{device}")
+    t = torch.tensor([value], dtype=torch.float64, device="cpu" if device is None else f"cuda:{device}")
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
 
-def barrier(pg, device: int):
+def barrier(pg, device):
     import torch
 
     if pg is not None:
         pg.barrier()
-    torch.cuda.synchronize(device)
+    if device is not None:
+        torch.cuda.synchronize(device)
+
+
+def replica_value(world: int, updates_per_rank: int, max_ms: float) -> float:
+    """Whole-job GLL-point-updates/s of N replicas: every rank did the same
+    work; the slowest rank's device time bounds the job."""
+    return world * updates_per_rank / (max_ms * 1e-3)
 
 
 def _cpu_env():
@@ -275,7 +287,7 @@ def bench_config3(args, world, rank, device, pg, headline: bool) -> dict:
     hbm, how = peaks()
     b_step = prob.algorithmic_bytes_per_step()
     achieved = b_step / (ms * 1e-3 / steps) / 1e9
-    out = {"value": world * points * steps / (ms * 1e-3), "ms_per_step": ms / steps, "steps": steps,
+    out = {"value": replica_value(world, points * steps, ms), "ms_per_step": ms / steps, "steps": steps,
            "workload": f"config3 coupled 2D Cartesian {args.nx}x{args.nx} order 5 (water over 8 curved elastic layers)",
            "points": points, "elements": prob.n_elements_total(), "setup_seconds": round(setup_s, 1),
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
@@ -343,7 +355,7 @@ def bench_config4(args, world, rank, device, pg) -> dict:
         plain_ms += s.last_advance_ms
         plain_updates += prob.n_global_total() * args.plain_steps
     plain_ms = reduce_max(pg, plain_ms, device)
-    plain_value = world * plain_updates / (plain_ms * 1e-3)
+    plain_value = replica_value(world, plain_updates, plain_ms)
 
     # batched
     batch = pkg.Batch(device=device, use_graphs=not args.no_graphs)
@@ -355,7 +367,7 @@ def bench_config4(args, world, rank, device, pg) -> dict:
         barrier(pg, device)
     updates = batch.point_updates
     ms = reduce_max(pg, batch.last_advance_ms, device)
-    value = world * updates / (ms * 1e-3)
+    value = replica_value(world, updates, ms)
     kps = batch.kernels_per_step if not args.no_graphs else None
 
     line_e2e = None
