@@ -9,7 +9,9 @@ Its best size depends on the class:
 
 The library starts from an occupancy-based choice. This module times
 candidate sizes around that choice on real problems, one class at a time,
-with the other classes held. It keeps the fastest and registers it
+with the other classes held: ``tune`` on solo solves, ``tune_batched`` on the
+tile launches of a batch of the class's largest problems (the setting of the
+batched workload). It keeps the fastest and registers it
 process-wide (``insem_cuda_set_tile_elements``), so solvers built afterwards
 use it. Tables can be saved as JSON and loaded again.
 """
@@ -90,6 +92,45 @@ def tune(problems: Iterable[ProblemData], device: int = 0, warmup: int = 3, step
     return out
 
 
+def tune_batched(problems: Iterable[ProblemData], device: int = 0, reps: int = 2, warmup: int = 3, steps: int = 6,
+                 min_share: float = 0.05, verbose: bool = False) -> Dict[ClassKey, dict]:
+    """Tunes the classes that hold at least `min_share` of the problems'
+    elements, in the setting they run in: the `reps` largest problems of the
+    class are built into a batch at every candidate size, and the batch's
+    tile launches are timed with CUDA events (Batch.profile).  The other
+    classes keep their current choice.  Registers and returns the choices."""
+    from .batch import Batch
+
+    problems = list(problems)
+    weight: Dict[ClassKey, int] = {}
+    members: Dict[ClassKey, List[ProblemData]] = {}
+    for p in problems:
+        for key, d in zip(classes_of(p), p.domains):
+            weight[key] = weight.get(key, 0) + d.n_elements
+            members.setdefault(key, []).append(p)
+    total = sum(weight.values()) or 1
+    out: Dict[ClassKey, dict] = {}
+    for key in sorted(weight, key=lambda k: -weight[k]):
+        if weight[key] < min_share * total:
+            continue
+        group = sorted(members[key], key=lambda p: -p.n_elements_total())[:reps]
+        timings = {}
+        for te in candidates(key):
+            register(key, te)
+            with Batch(device=device) as b:
+                for prob in group:
+                    b.adopt(Solver(prob, device=device))
+                b.advance(warmup)
+                tile_ms, _ = b.profile(steps)
+            timings[te] = tile_ms / steps
+            if verbose:
+                print(f"  class {key} te={te}: {timings[te]:.4f} ms of tile launches per step", flush=True)
+        best = min(timings, key=timings.get)
+        register(key, best)
+        out[key] = {"te": best, "ms": timings[best], "timings": timings, "share": weight[key] / total}
+    return out
+
+
 def save(table: Dict[ClassKey, dict], path: str) -> None:
     rows = [{"class": list(k), "te": v["te"], "ms": v.get("ms"), "timings": v.get("timings")} for k, v in table.items()]
     with open(path, "w") as f:
@@ -113,4 +154,5 @@ def summary(table: Optional[Dict[ClassKey, dict]]) -> list:
         return []
     names = {N.RECT: "rect", N.AFFINE: "affine", N.CURVED: "curved", N.AXISYM: "axisym"}
     return [{"ngll": k[0], "kind": names.get(k[1], k[1]), "medium": "elastic" if k[2] == N.ELASTIC else "acoustic",
-             "m": k[3], "te": v["te"], "ms_per_step": round(v["ms"], 5)} for k, v in sorted(table.items())]
+             "m": k[3], "te": v["te"], "ms_per_step": round(v["ms"], 5),
+             **({"share": round(v["share"], 3)} if "share" in v else {})} for k, v in sorted(table.items())]

@@ -34,6 +34,7 @@ static __global__ void batch_row_gather_kernel(const StreamSeg* __restrict__ seg
 void Solver::batch_prepare() {
   DeviceGuard dg(device);
   INSEM_REQUIRE(tiled, INSEM_CUDA_ERR_STATE, "batched solves run on the tiled path");
+  if (in_batch) return;  // prepared already
   if (!initialized) {
     set_mode(kModeInit);
     enqueue_tiled(parity, true);
@@ -230,11 +231,12 @@ int32_t Batch::adopt(insem_cuda_solver* h) {
   INSEM_REQUIRE(h && h->s, INSEM_CUDA_ERR_INVALID, "null solve");
   INSEM_REQUIRE(h->s->tiled, INSEM_CUDA_ERR_INVALID, "batched solves run on the tiled path");
   INSEM_REQUIRE(h->s->device == opts.device, INSEM_CUDA_ERR_INVALID, "the solve lives on another device");
-  INSEM_REQUIRE(!h->s->in_batch, INSEM_CUDA_ERR_STATE, "the solve belongs to a batch");
+  INSEM_REQUIRE(!h->s->batch_owner, INSEM_CUDA_ERR_STATE, "the solve belongs to a batch");
   for (const auto& m : members) INSEM_REQUIRE(m.get() != h, INSEM_CUDA_ERR_STATE, "the solve belongs to this batch");
   int64_t pts = 0;
   for (const auto& d : h->s->domains) pts += d.ng;
   members.emplace_back(h);
+  h->s->batch_owner = this;
   prepared.push_back(0);
   member_points.push_back(pts);
   dirty = true;
@@ -296,8 +298,8 @@ void Batch::rebuild() {
     d.kind = c.kind;
     d.m = c.m;
     d.elastic = c.elastic;
-    d.segs.upload(c.segs);
-    d.items.upload(c.items);
+    d.segs.upload_async(c.segs, stream);
+    d.items.upload_async(c.items, stream);
     d.n_items = static_cast<int32_t>(c.items.size());
     d.te = c.te;
     d.L = TileLayout::make(c.ngll, c.ncomp, c.kind, c.elastic, c.te, c.tp_cap, c.nc_cap);
@@ -312,31 +314,31 @@ void Batch::rebuild() {
     d.grid = std::max(1, std::min(d.n_items, per_sm * n_sms));
     dclasses.push_back(std::move(d));
   }
-  queues.resize(std::max<std::size_t>(dclasses.size(), 1));
+  if (queues.size() != std::max<std::size_t>(dclasses.size(), 1)) queues.resize(std::max<std::size_t>(dclasses.size(), 1));
   queues.zero(stream);
   for (int c = 0; c < 3; ++c) {
-    dhalo_segs[c].upload(T.halo_segs[c]);
-    dhalo_items[c].upload(T.halo_items[c]);
+    dhalo_segs[c].upload_async(T.halo_segs[c], stream);
+    dhalo_items[c].upload_async(T.halo_items[c], stream);
     n_halo_items[c] = static_cast<int32_t>(T.halo_items[c].size());
   }
-  dcons_segs.upload(T.cons_segs);
-  dcons_items.upload(T.cons_items);
+  dcons_segs.upload_async(T.cons_segs, stream);
+  dcons_items.upload_async(T.cons_items, stream);
   n_cons_items = static_cast<int32_t>(T.cons_items.size());
-  drec_segs.upload(T.rec_segs);
-  dpv_items.upload(T.pv_items);
-  drec_items.upload(T.rec_items);
+  drec_segs.upload_async(T.rec_segs, stream);
+  dpv_items.upload_async(T.pv_items, stream);
+  drec_items.upload_async(T.rec_items, stream);
   n_pv_items = static_cast<int32_t>(T.pv_items.size());
   n_rec_items = static_cast<int32_t>(T.rec_items.size());
-  denergy.upload(T.energy_segs);
+  denergy.upload_async(T.energy_segs, stream);
   n_energy = static_cast<int32_t>(T.energy_segs.size());
-  dstates.upload(T.states);
+  dstates.upload_async(T.states, stream);
   n_states = static_cast<int32_t>(T.states.size());
-  dstream.upload(T.stream_segs);
+  dstream.upload_async(T.stream_segs, stream);
   n_stream = static_cast<int32_t>(T.stream_segs.size());
   amp_cols = T.amp_cols;
   row_cols = T.row_cols;
-  amp_stage.resize(std::max(amp_cols, 1));
-  row_stage.resize(std::max(row_cols, 1));
+  if (amp_stage.size() < static_cast<std::size_t>(std::max(amp_cols, 1))) amp_stage.resize(std::max(amp_cols, 1));
+  if (row_stage.size() < static_cast<std::size_t>(std::max(row_cols, 1))) row_stage.resize(std::max(row_cols, 1));
   CUDA_CHECK(cudaStreamSynchronize(stream));
   if (opts.use_graphs && n_states > 0) {
     cudaGraph_t g = nullptr;
@@ -561,6 +563,13 @@ struct insem_cuda_batch {
 };
 
 extern "C" {
+
+int insem_cuda_solver_prepare_for_batch(insem_cuda_solver* h) {
+  return guarded([&] {
+    INSEM_REQUIRE(h, INSEM_CUDA_ERR_INVALID, "null handle");
+    h->s->batch_prepare();
+  });
+}
 
 int insem_cuda_batch_create(const insem_cuda_options* options, insem_cuda_batch** out) {
   return guarded([&] {

@@ -154,6 +154,29 @@ class DeviceBuffer {
     }
   }
   void upload(const std::vector<T>& v) { upload(v.data(), v.size()); }
+  // For buffers only stream `s` uses: (re)allocates from the pool and copies
+  // in s's order, without waiting for the legacy stream (a new size frees the
+  // old memory, which `s` must no longer be using).
+  void upload_async(const std::vector<T>& v, cudaStream_t s) {
+    if (v.size() != n_) {
+      release();
+      if (!v.empty()) {
+        int device = 0;
+        CUDA_CHECK(cudaGetDevice(&device));
+        keep_pool_memory(device);
+        void* p = nullptr;
+        const cudaError_t e = cudaMallocAsync(&p, v.size() * sizeof(T), s);
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          throw Error(INSEM_CUDA_ERR_NOMEM, "device allocation of " + std::to_string(v.size() * sizeof(T)) +
+                                                " bytes failed: " + cudaGetErrorString(e));
+        }
+        p_ = static_cast<T*>(p);
+        n_ = v.size();
+      }
+    }
+    if (!v.empty()) CUDA_CHECK(cudaMemcpyAsync(p_, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
   void zero(cudaStream_t s = nullptr) {
     if (n_) CUDA_CHECK(cudaMemsetAsync(p_, 0, n_ * sizeof(T), s));
   }

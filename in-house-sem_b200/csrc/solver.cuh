@@ -146,7 +146,8 @@ class Solver {
 
   // ------------------------------------------------------ batched stepping
  public:
-  bool in_batch = false;  // stepped by a Batch; advance() refuses
+  bool in_batch = false;        // prepared for batched steps; advance() refuses
+  const void* batch_owner = nullptr;  // the Batch that owns this solve
   int32_t remaining() const { return n_steps - step; }
   // Runs the initial step (if not yet run) and the predictor, leaving the
   // fields ready for a normal step; primes the StepState's parity and last step.

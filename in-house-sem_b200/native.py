@@ -144,6 +144,7 @@ def lib() -> C.CDLL:
             "insem_cuda_batch_destroy": (None, [vp]),
             "insem_cuda_batch_add": (C.c_int, [vp, C.POINTER(Problem), i32p]),
             "insem_cuda_batch_adopt": (C.c_int, [vp, vp, i32p]),
+            "insem_cuda_solver_prepare_for_batch": (C.c_int, [vp]),
             "insem_cuda_batch_advance": (C.c_int, [vp, C.c_int32]),
             "insem_cuda_batch_run": (C.c_int, [vp]),
             "insem_cuda_batch_remove": (C.c_int, [vp, C.c_int32]),

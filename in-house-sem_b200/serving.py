@@ -179,10 +179,14 @@ def _stage_host(req: Request):
     return model, arrays, ne, device_bytes_estimate(ProblemData.from_npz(probe))
 
 
-def _stage_device(model, arrays, device: int, use_graphs: bool):
-    """Stage B (device, worker thread): dt from the power iteration, the solver."""
+def _stage_device(model, arrays, device: int, use_graphs: bool, prepare: bool):
+    """Stage B (device, worker thread): dt from the power iteration, the solver
+    (and, for the batched server, its initial step and predictor)."""
     prob = K.build_from_arrays(model, arrays, device=device)
-    return prob, Solver(prob, device=device, use_graphs=use_graphs)
+    s = Solver(prob, device=device, use_graphs=use_graphs)
+    if prepare:
+        s.prepare_for_batch()
+    return prob, s
 
 
 class _Pipeline:
@@ -190,9 +194,10 @@ class _Pipeline:
     Solvers come out in arrival order, ready to step."""
 
     def __init__(self, stream: List[Request], recs: Dict[int, Record], device: int, budget: int, workers: int,
-                 use_graphs: bool):
+                 use_graphs: bool, prepare: bool):
         self.stream, self.recs, self.device, self.budget = stream, recs, device, budget
         self.use_graphs = use_graphs
+        self.prepare = prepare
         self.pool = ThreadPoolExecutor(max_workers=workers)
         self.host: Dict[int, object] = {}     # rid -> future of stage A
         self.waiting: deque = deque()        # (rid, model, arrays, bytes), arrival order
@@ -231,7 +236,7 @@ class _Pipeline:
             self.used += need
             self.recs[rid].admitted = self.now()
             self.dev.append((rid, need, self.pool.submit(_stage_device, model, arrays, self.device,
-                                                         self.use_graphs)))
+                                                         self.use_graphs, self.prepare)))
         out = []
         while self.dev and self.dev[0][2].done():
             rid, need, f = self.dev.popleft()
@@ -258,7 +263,7 @@ class _Pipeline:
 class Server:
     """Continuous-batching server over one Batch on one device."""
 
-    def __init__(self, device: int = 0, hbm_budget: Optional[int] = None, chunk_steps: int = 32,
+    def __init__(self, device: int = 0, hbm_budget: Optional[int] = None, chunk_steps: int = 64,
                  workers: Optional[int] = None, use_graphs: bool = True):
         import os
 
@@ -272,7 +277,7 @@ class Server:
     def run(self, stream: List[Request], keep_traces: bool = True) -> Dict[int, Record]:
         recs = {r.rid: Record(r.rid, r.kind, r.arrival) for r in stream}
         batch = Batch(device=self.device, use_graphs=self.use_graphs)
-        pipe = _Pipeline(stream, recs, self.device, self.budget, self.workers, self.use_graphs)
+        pipe = _Pipeline(stream, recs, self.device, self.budget, self.workers, self.use_graphs, True)
         members: Dict[int, tuple] = {}    # batch index -> (rid, member, bytes, streamed row blocks)
         try:
             while pipe.pending() or members:
@@ -320,7 +325,7 @@ def serve_plain(stream: List[Request], device: int = 0, workers: Optional[int] =
     recs = {r.rid: Record(r.rid, r.kind, r.arrival) for r in stream}
     free, _ = mem_info(device)
     pipe = _Pipeline(stream, recs, device, int(hbm_budget) if hbm_budget else int(0.8 * free),
-                     workers or max(1, min(32, os.cpu_count() or 1)), True)
+                     workers or max(1, min(32, os.cpu_count() or 1)), True, False)
     ready: deque = deque()
     try:
         while pipe.pending() or ready:

@@ -79,6 +79,12 @@ class Solver:
     def run(self) -> None:
         N.check(N.lib().insem_cuda_solver_run(self._h))
 
+    def prepare_for_batch(self) -> None:
+        """Runs the initial step and the predictor now (on this solver's
+        stream), so that joining a batch later costs the batch nothing;
+        afterwards only a batch steps this solver."""
+        N.check(N.lib().insem_cuda_solver_prepare_for_batch(self._h))
+
     def advance_streamed(self, n_steps: int, amplitudes: np.ndarray, rows_out: np.ndarray) -> int:
         """n steps with per-step source amplitudes in ([n][n_sources] float32, host) and
         the recorded rows out ([>= n / record_every][n_columns] float64, host)."""

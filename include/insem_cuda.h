@@ -344,7 +344,11 @@ int insem_cuda_batch_create(const insem_cuda_options* options, insem_cuda_batch*
 void insem_cuda_batch_destroy(insem_cuda_batch* h);
 /* Builds a solve (device upload) and appends it; *index (may be NULL) is its index. */
 int insem_cuda_batch_add(insem_cuda_batch* h, const insem_cuda_problem* problem, int32_t* index);
-/* Takes ownership of a solver handle that has not been stepped by a batch. */
+/* Runs what joining a batch needs (the initial step and the predictor) now,
+ * on the solver's own stream, so that a later add to a batch costs nothing on
+ * the batch's stream.  Afterwards only a batch steps the solver. */
+int insem_cuda_solver_prepare_for_batch(insem_cuda_solver* h);
+/* Takes ownership of a solver handle that no batch owns (prepared or not). */
 int insem_cuda_batch_adopt(insem_cuda_batch* h, insem_cuda_solver* solver, int32_t* index);
 /* n batched steps (fewer if every member ends sooner); a member with fewer
  * steps left runs its last step in final mode and then idles: the batch's
