@@ -33,6 +33,35 @@ namespace insem_b200 {
 // GLL derivative matrix, GLJ derivative matrix and w_i w_j per ngll (2..9).
 static __constant__ float c_basis[8][3][81];
 
+// Both components of an interleaved pair in one 64-bit shared-memory load.
+// (The sums stay scalar: Blackwell's two-lane FP32 multiply and add each
+// round like the scalar instructions, but the assembler fuses a two-lane
+// multiply feeding a two-lane add into one fused operation, which rounds
+// once; the reference rounds the product and the sum separately.)
+__device__ __forceinline__ float2 pair_load(const float* p) { return *reinterpret_cast<const float2*>(p); }
+
+// Element stride (floats) of the field / xi-flux rows in shared memory.
+// Two components are stored interleaved, row j of element e at
+// e * stride + j * 2 * ngll, (l, c) at + 2 l + c, so one 64-bit load gives
+// both; the stride is padded so that the elements one warp reads fall on
+// distinct 64-bit bank pairs.  Other component counts keep
+// [component][row][ROW].
+__host__ __device__ constexpr int rows_elem_stride(int ng, int nc) {
+  if (nc != 2) return nc * ng * ((ng + 1) & ~1);
+  const int base = 2 * ng * ng;
+  const int per_warp = 32 / ng + 2;
+  for (int s = base; s < base + 64; s += 2) {
+    bool ok = true;
+    for (int a = 0; a < per_warp && ok; ++a)
+      for (int b = a + 1; b < per_warp && ok; ++b) {
+        const int da = (a * s) % 32, db = (b * s) % 32;
+        if (da == db || (da + 1) % 32 == db || (db + 1) % 32 == da) ok = false;
+      }
+    if (ok) return s;
+  }
+  return base;
+}
+
 // kModeIdle: a batched solve past its last step (the batch's kernels skip it).
 enum StepMode : int32_t { kModeNormal = 0, kModeFinal = 1, kModeInit = 2, kModeIdle = 3 };
 
@@ -184,9 +213,11 @@ struct TileLayout {
     L.tf = o;
     o = up16(o + 4u * nc * tp_cap);
     L.su = o;
-    o = up16(o + 4u * te * nc * ng * L.row);
+    const uint32_t rows = static_cast<uint32_t>(rows_elem_stride(ng, nc));
+    // su doubles as the halo staging area: [te][nc][npe]
+    o = up16(o + 4u * te * (rows > static_cast<uint32_t>(nc * npe) ? rows : static_cast<uint32_t>(nc * npe)));
     L.sfx = o;
-    o = up16(o + 4u * te * nc * ng * L.row);
+    o = up16(o + 4u * te * rows);
     L.ax = o;
     if (axi) o = up16(o + 4u * te * 64);
     L.total = o;
@@ -341,8 +372,12 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   const int i = tid - el * NG;
   const bool active = el < th.ne;
   const uint32_t* desc = s_desc + el * CS;
-  float* urow = su + el * (NC * NG * ROW);
-  float* frow = sfx + el * (NC * NG * ROW);
+  constexpr int ES = rows_elem_stride(NG, NC);  // element stride of the rows
+  constexpr bool PAIR = NC == 2;                 // interleaved components, two-lane sums
+  // position of (component c, row j, column l) in an element's rows
+  auto ridx = [](int c, int j, int l) { return PAIR ? j * 2 * NG + 2 * l + c : (c * NG + j) * ROW + l; };
+  float* urow = su + el * ES;
+  float* frow = sfx + el * ES;
   float* ax = sax + el * 64;
 
   // 2. element field rows (slots through their tile point or the constrained list)
@@ -353,8 +388,12 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       dsc[j] = desc[j * NG + i];
       if (!(dsc[j] & kSlotConstrained)) {
         const int p = dsc[j] & kSlotPointMask;
+        if constexpr (PAIR) {
+          *reinterpret_cast<float2*>(urow + ridx(0, j, i)) = make_float2(tu[p], tu[tp_cap + p]);
+        } else {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) urow[(c * NG + j) * ROW + i] = tu[c * tp_cap + p];
+          for (int c = 0; c < NC; ++c) urow[ridx(c, j, i)] = tu[c * tp_cap + p];
+        }
       }
     }
   }
@@ -365,7 +404,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     const int jj = k / NG, ii = k - jj * NG;
 #pragma unroll
     for (int c = 0; c < NC; ++c)
-      su[e * (NC * NG * ROW) + (c * NG + jj) * ROW + ii] = td.cval[static_cast<size_t>(c) * td.n_cslots + ci];
+      su[e * ES + ridx(c, jj, ii)] = td.cval[static_cast<size_t>(c) * td.n_cslots + ci];
   }
   __syncthreads();
 
@@ -380,38 +419,72 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   }
   float ucol[NC][NG], fe[NC][NG], dir[2][NG];
   if (active) {
+    if constexpr (PAIR) {
+      // column i of both components, one 64-bit load per row
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
+      for (int l = 0; l < NG; ++l) {
+        const float2 v = pair_load(urow + ridx(0, l, i));
+        ucol[0][l] = v.x;
+        ucol[1][l] = v.y;
+      }
 #pragma unroll
-      for (int j = 0; j < NG; ++j) ucol[c][j] = urow[(c * NG + j) * ROW + i];
-#pragma unroll
-    for (int j = 0; j < NG; ++j) {
-      const int k = j * NG + i;
-      float uxi[NC], ueta[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const float* row = urow + (c * NG + j) * ROW;
-        float a = 0.0f, b = 0.0f;
+      for (int j = 0; j < NG; ++j) {
+        const int k = j * NG + i;
+        const float* row = urow + ridx(0, j, 0);
+        float a0 = 0.0f, a1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
 #pragma unroll
         for (int l = 0; l < NG; ++l) {
-          a = fadd(a, fmul(dxr[l], row[l]));
-          b = fadd(b, fmul(cbasis(NG, 0, j * NG + l), ucol[c][l]));
+          const float2 r = pair_load(row + 2 * l);
+          const float d = cbasis(NG, 0, j * NG + l);
+          a0 = fadd(a0, fmul(dxr[l], r.x));
+          a1 = fadd(a1, fmul(dxr[l], r.y));
+          b0 = fadd(b0, fmul(d, ucol[0][l]));
+          b1 = fadd(b1, fmul(d, ucol[1][l]));
         }
-        uxi[c] = a;
-        ueta[c] = b;
+        float uxi[NC] = {a0, a1}, ueta[NC] = {b0, b1}, upt[NC] = {ucol[0][j], ucol[1][j]};
+        float fx[NC], fy[NC], dr[2] = {0.0f, 0.0f};
+        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
+                                    w2c[j]);
+        *reinterpret_cast<float2*>(frow + ridx(0, j, i)) = make_float2(fx[0], fx[1]);
+        fe[0][j] = fy[0];
+        fe[1][j] = fy[1];
+        dir[0][j] = dr[0];
+        dir[1][j] = dr[1];
       }
-      float fx[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
+    } else {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
-      point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
-                                  w2c[j]);
+      for (int c = 0; c < NC; ++c)
 #pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        frow[(c * NG + j) * ROW + i] = fx[c];
-        fe[c][j] = fy[c];
+        for (int j = 0; j < NG; ++j) ucol[c][j] = urow[ridx(c, j, i)];
+#pragma unroll
+      for (int j = 0; j < NG; ++j) {
+        const int k = j * NG + i;
+        float uxi[NC], ueta[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float* row = urow + ridx(c, j, 0);
+          float a = 0.0f, b = 0.0f;
+#pragma unroll
+          for (int l = 0; l < NG; ++l) {
+            a = fadd(a, fmul(dxr[l], row[l]));
+            b = fadd(b, fmul(cbasis(NG, 0, j * NG + l), ucol[c][l]));
+          }
+          uxi[c] = a;
+          ueta[c] = b;
+        }
+        float fx[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
+        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
+                                    w2c[j]);
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          frow[ridx(c, j, i)] = fx[c];
+          fe[c][j] = fy[c];
+        }
+        dir[0][j] = dr[0];
+        dir[1][j] = dr[1];
       }
-      dir[0][j] = dr[0];
-      dir[1][j] = dr[1];
     }
   }
   __syncthreads();
@@ -422,16 +495,32 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
       float s[NC];
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        const float* row = frow + (c * NG + j) * ROW;
-        float acc = 0.0f;
+      if constexpr (PAIR) {
+        const float* row = frow + ridx(0, j, 0);
+        float acc0 = 0.0f, acc1 = 0.0f;
 #pragma unroll
         for (int l = 0; l < NG; ++l) {
-          acc = fadd(acc, fmul(dxc[l], row[l]));
-          acc = fadd(acc, fmul(cbasis(NG, 0, l * NG + j), fe[c][l]));
+          const float2 r = pair_load(row + 2 * l);
+          const float d = cbasis(NG, 0, l * NG + j);
+          acc0 = fadd(acc0, fmul(dxc[l], r.x));
+          acc0 = fadd(acc0, fmul(d, fe[0][l]));
+          acc1 = fadd(acc1, fmul(dxc[l], r.y));
+          acc1 = fadd(acc1, fmul(d, fe[1][l]));
         }
-        s[c] = acc;
+        s[0] = acc0;
+        s[1] = acc1;
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+          const float* row = frow + ridx(c, j, 0);
+          float acc = 0.0f;
+#pragma unroll
+          for (int l = 0; l < NG; ++l) {
+            acc = fadd(acc, fmul(dxc[l], row[l]));
+            acc = fadd(acc, fmul(cbasis(NG, 0, l * NG + j), fe[c][l]));
+          }
+          s[c] = acc;
+        }
       }
       const float drj[2] = {dir[0][j], dir[1][j]};
       float out[NC];
