@@ -131,9 +131,11 @@ __device__ __forceinline__ float cbasis(int ng, int which, int idx) { return c_b
 
 
 // ------------------------------------------------------- bulk-copy helpers
-// One mbarrier per CTA tracks the tile's bulk copies (cp.async.bulk, the
-// non-tensor TMA path): thread 0 announces the byte count and issues the
-// copies; every thread waits on the barrier's phase 0.
+// Two mbarriers per CTA track the tile's bulk copies (cp.async.bulk, the
+// non-tensor TMA path), one for the copies at the start of a tile and one
+// for the late copies: thread 0 announces the byte count and issues the
+// copies; every thread waits on the barrier's current phase (the persistent
+// kernel's tiles alternate the phase).
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -149,6 +151,11 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
       "l"(src), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
+}
+// Orders this thread's earlier generic-proxy accesses to shared memory (made
+// visible to it by a block barrier) before bulk copies that overwrite them.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -171,11 +178,13 @@ constexpr uint32_t kBulkWaitLimit = 1u << 22;
 // Shared-memory layout of one tile CTA, byte offsets (16-byte aligned).
 // Per-tile data arrives by bulk copies: element data (metric, coefficients,
 // axisymmetric weights), slot descriptors, and the complete points' u, v
-// and inverse mass; halo tile points are gathered by the threads into the u
-// region after the complete points (at index roundup(nc, 4) on).
+// and inverse mass (v and 1/M later, when `late`); halo tile points are
+// gathered by the threads into the u region after the complete points (at
+// index roundup(nc, 4) on).
 struct TileLayout {
   uint32_t bar, metric, coef0, coef1, wr, hoop, r, desc, u, v, im, tf, su, sfx, ax, total;
   int32_t tp_cap, nc_cap, ms, cs, row;
+  int32_t late;  // 1: v and 1/M arrive by a second copy into the element-data region
 
   __host__ __device__ static uint32_t up16(uint32_t x) { return (x + 15u) & ~15u; }
   __host__ __device__ static TileLayout make(int ng, int nc, int kind, bool elastic, int te, int tp_cap, int nc_cap) {
@@ -188,8 +197,8 @@ struct TileLayout {
     L.nc_cap = nc_cap;
     const bool axi = kind == INSEM_AXISYM;
     uint32_t o = 0;
-    L.bar = o;
-    o = up16(o + 8);
+    L.bar = o;  // two mbarriers: the tile's copies, the late v and 1/M copies
+    o = up16(o + 16);
     L.metric = o;
     o = up16(o + 4u * te * L.ms);
     L.coef0 = o;
@@ -204,20 +213,31 @@ struct TileLayout {
     if (axi) o = up16(o + 4u * te * L.cs);
     L.desc = o;
     o = up16(o + 4u * te * L.cs);
+    // The element data [metric, elem_end) is last read by the fluxes.  The
+    // f_xi rows (written after the fluxes, read by the divergence) and then
+    // the assembly target with v and 1/M (copied in after the divergence)
+    // reuse that region when it is large enough.
+    const uint32_t elem = o - L.metric;
     L.u = o;
-    o = up16(o + 4u * nc * tp_cap);
-    L.v = o;
-    o = up16(o + 4u * nc * nc_cap);
-    L.im = o;
-    o = up16(o + 4u * nc_cap);
-    L.tf = o;
     o = up16(o + 4u * nc * tp_cap);
     L.su = o;
     const uint32_t rows = static_cast<uint32_t>(rows_elem_stride(ng, nc));
     // su doubles as the halo staging area: [te][nc][npe]
     o = up16(o + 4u * te * (rows > static_cast<uint32_t>(nc * npe) ? rows : static_cast<uint32_t>(nc * npe)));
-    L.sfx = o;
-    o = up16(o + 4u * te * rows);
+    const uint32_t sfx_b = up16(4u * te * rows);
+    if (sfx_b <= elem) {
+      L.sfx = L.metric;
+    } else {
+      L.sfx = o;
+      o += sfx_b;
+    }
+    const uint32_t tf_b = up16(4u * nc * tp_cap), v_b = up16(4u * nc * nc_cap), im_b = up16(4u * nc_cap);
+    L.late = tf_b + v_b + im_b <= elem ? 1 : 0;
+    uint32_t p = L.late ? L.metric : o;
+    L.tf = p;
+    L.v = p + tf_b;
+    L.im = p + tf_b + v_b;
+    if (!L.late) o += tf_b + v_b + im_b;
     L.ax = o;
     if (axi) o = up16(o + 4u * te * 64);
     L.total = o;
@@ -321,11 +341,13 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   const bool energy = (mode == kModeInit) ? (sc.energy_every > 0) : (sc.energy_every > 0 && step % sc.energy_every == 0);
   const int nc4 = (th.nc + 3) & ~3;
 
-  // 1. bulk copies of the tile's element data, slot descriptors and complete points
+  // 1. bulk copies of the tile's element data, slot descriptors and complete
+  //    points (u; v and 1/M too unless they come late)
   if (tid == 0) {
     const uint32_t eb = 4u * th.ne;
     uint32_t total = eb * MS + eb * CS * (1 + (EL ? 1 : 0) + (AXI ? 3 : 0)) + eb * CS;
-    if (nc4 > 0) total += 4u * nc4 * (2 * NC + 1);
+    if (nc4 > 0) total += 4u * nc4 * (L.late ? NC : 2 * NC + 1);
+    fence_proxy_async_smem();
     mbar_expect_tx(bar, total);
     bulk_load(s_metric, blk.metric + static_cast<size_t>(th.be0) * MS, eb * MS, bar);
     bulk_load(s_coef0, blk.coef0 + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
@@ -340,9 +362,9 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         bulk_load(tu + c * tp_cap, td.u_cur + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar);
-        bulk_load(s_v + c * nc_cap, td.v + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar);
+        if (!L.late) bulk_load(s_v + c * nc_cap, td.v + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar);
       }
-      bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar);
+      if (!L.late) bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar);
     }
   }
   // halo tile points, gathered while the bulk copies are in flight
@@ -417,7 +439,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     dxc[l] = cbasis(NG, axial ? 1 : 0, l * NG + i);
     w2c[l] = cbasis(NG, 2, l * NG + i);
   }
-  float ucol[NC][NG], fe[NC][NG], dir[2][NG];
+  float ucol[NC][NG], fe[NC][NG], fx[NC][NG], dir[2][NG];  // fx: f_xi column, stored after the barrier
   if (active) {
     if constexpr (PAIR) {
       // column i of both components, one 64-bit load per row
@@ -442,10 +464,11 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
           b1 = fadd(b1, fmul(d, ucol[1][l]));
         }
         float uxi[NC] = {a0, a1}, ueta[NC] = {b0, b1}, upt[NC] = {ucol[0][j], ucol[1][j]};
-        float fx[NC], fy[NC], dr[2] = {0.0f, 0.0f};
-        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
+        float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f};
+        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + 16, ax + 32, ax + 48,
                                     w2c[j]);
-        *reinterpret_cast<float2*>(frow + ridx(0, j, i)) = make_float2(fx[0], fx[1]);
+        fx[0][j] = fxp[0];
+        fx[1][j] = fxp[1];
         fe[0][j] = fy[0];
         fe[1][j] = fy[1];
         dir[0][j] = dr[0];
@@ -472,18 +495,30 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
           uxi[c] = a;
           ueta[c] = b;
         }
-        float fx[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
+        float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
-        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fx, fy, dr, ax, ax + 16, ax + 32, ax + 48,
+        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + 16, ax + 32, ax + 48,
                                     w2c[j]);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          frow[ridx(c, j, i)] = fx[c];
+          fx[c][j] = fxp[c];
           fe[c][j] = fy[c];
         }
         dir[0][j] = dr[0];
         dir[1][j] = dr[1];
+      }
+    }
+  }
+  __syncthreads();  // the element data is dead: the f_xi rows may overwrite it
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < NG; ++j) {
+      if constexpr (PAIR) {
+        *reinterpret_cast<float2*>(frow + ridx(0, j, i)) = make_float2(fx[0][j], fx[1][j]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NC; ++c) frow[ridx(c, j, i)] = fx[c][j];
       }
     }
   }
@@ -530,7 +565,20 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       for (int c = 0; c < NC; ++c) fo[c][j] = out[c];
     }
   }
-  __syncthreads();  // su is reused below as halo staging
+  __syncthreads();  // su is reused below as halo staging; the f_xi rows are dead
+
+  // v and 1/M of the complete points, into the element-data region behind the
+  // assembly target, while the assembly runs
+  if (L.late && tid == 0) {
+    fence_proxy_async_smem();
+    mbar_expect_tx(bar + 1, nc4 > 0 ? 4u * nc4 * (NC + 1) : 0u);
+    if (nc4 > 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        bulk_load(s_v + c * nc_cap, td.v + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar + 1);
+      bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar + 1);
+    }
+  }
 
   // 5. local assembly in the reference's slot order, halo staging
   float* stage = su;
@@ -569,6 +617,15 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 #pragma unroll
     for (int c = 0; c < NC; ++c)
       td.hbuf[static_cast<size_t>(c) * td.n_hbuf + th.hb + q] = stage[(e * NC + c) * NPE + k];
+  }
+
+  if (L.late) {
+    const bool late_arrived = mbar_wait_bounded(bar + 1, phase, kBulkWaitLimit);
+    if (__syncthreads_or(!late_arrived)) {
+      if (tid == 0) atomicExch(&st->error, 1);
+      mbar_wait_bounded(bar + 1, phase, kBulkWaitLimit);
+      return false;
+    }
   }
 
   // 7. complete points: a = f / M, corrector, predictor; energy partials
@@ -628,7 +685,10 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
                      double* __restrict__ epartial, int32_t tile0, TileLayout L) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + L.bar);
-  if (threadIdx.x == 0) mbar_init(bar, 1);
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+  }
   __syncthreads();
   tile_step_body<NG, KIND, EL, M>(blk, td, sc, st, epartial, tile0 + blockIdx.x, L, smem_raw, bar, 0u);
 }
@@ -652,11 +712,14 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
     tile_batch_kernel(const TileSeg* __restrict__ segs, const int2* __restrict__ items, int32_t n_items,
                       int32_t* __restrict__ queue, TileLayout L) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar[2];
   __shared__ __align__(16) TileSeg s_seg;  // the item's segment, read by the body from shared memory
   __shared__ int32_t s_item, s_segi, s_tile, s_idle;
   static_assert(sizeof(TileSeg) % 4 == 0, "TileSeg is copied as 32-bit words");
-  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+  }
   __syncthreads();
   uint32_t phase = 0;
   for (;;) {
@@ -689,7 +752,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
     if (s_idle) continue;  // a finished solve: no copies issued, the barrier phase is unchanged
     const int32_t local = s_tile;
     const bool ok = tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial,
-                                                    s_seg.tile0 + local, L, smem_raw, &bar, phase);
+                                                    s_seg.tile0 + local, L, smem_raw, bar, phase);
     if (!ok) break;
     phase ^= 1u;
     __syncthreads();  // the next item's copies overwrite shared memory
