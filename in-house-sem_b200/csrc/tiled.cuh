@@ -34,11 +34,39 @@ namespace insem_b200 {
 static __constant__ float c_basis[8][3][81];
 
 // Both components of an interleaved pair in one 64-bit shared-memory load.
-// (The sums stay scalar: Blackwell's two-lane FP32 multiply and add each
-// round like the scalar instructions, but the assembler fuses a two-lane
-// multiply feeding a two-lane add into one fused operation, which rounds
-// once; the reference rounds the product and the sum separately.)
 __device__ __forceinline__ float2 pair_load(const float* p) { return *reinterpret_cast<const float2*>(p); }
+
+// Two-lane FP32 arithmetic on a component pair (sm_100 add/fma .f32x2).  Each
+// lane rounds exactly like the scalar instruction.  The assembler fuses a
+// two-lane multiply that feeds a two-lane add into one fused multiply-add,
+// which rounds once where the reference rounds the product and the sum
+// separately; so a product is formed as fma(a, b, z) with z = -0 read from
+// constant memory at run time, which is exactly the rounded product (for
+// every a, b, including signed zeros) and is not fused further.
+static __constant__ float c_neg_zero;  // -0.0f, written with the basis
+using f2x = unsigned long long;        // two packed floats (lane 0 low)
+__device__ __forceinline__ f2x pk2(float x, float y) {
+  f2x r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(f2x r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+__device__ __forceinline__ f2x add2(f2x a, f2x b) {
+  f2x d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+// a * b rounded once per lane (nz = pk2(-0, -0) from c_neg_zero)
+__device__ __forceinline__ f2x mul2(f2x a, f2x b, f2x nz) {
+  f2x d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(nz));
+  return d;
+}
+__device__ __forceinline__ f2x pair_load2(const float* p) { return *reinterpret_cast<const f2x*>(p); }
 
 // Element stride (floats) of the field / xi-flux rows in shared memory.
 // Two components are stored interleaved, row j of element e at
@@ -442,10 +470,15 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   float ucol[NC][NG], fe[NC][NG], fx[NC][NG], dir[2][NG];  // fx: f_xi column, stored after the barrier
   if (active) {
     if constexpr (PAIR) {
-      // column i of both components, one 64-bit load per row
+      // column i of both components, one 64-bit load per row; both
+      // components' sums in two-lane instructions
+      const float nzs = c_neg_zero;
+      const f2x nz = pk2(nzs, nzs);
+      f2x uc[NG];
 #pragma unroll
       for (int l = 0; l < NG; ++l) {
-        const float2 v = pair_load(urow + ridx(0, l, i));
+        uc[l] = pair_load2(urow + ridx(0, l, i));
+        const float2 v = upk2(uc[l]);
         ucol[0][l] = v.x;
         ucol[1][l] = v.y;
       }
@@ -453,17 +486,15 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       for (int j = 0; j < NG; ++j) {
         const int k = j * NG + i;
         const float* row = urow + ridx(0, j, 0);
-        float a0 = 0.0f, a1 = 0.0f, b0 = 0.0f, b1 = 0.0f;
+        f2x a = 0ull, b = 0ull;  // (+0, +0)
 #pragma unroll
         for (int l = 0; l < NG; ++l) {
-          const float2 r = pair_load(row + 2 * l);
           const float d = cbasis(NG, 0, j * NG + l);
-          a0 = fadd(a0, fmul(dxr[l], r.x));
-          a1 = fadd(a1, fmul(dxr[l], r.y));
-          b0 = fadd(b0, fmul(d, ucol[0][l]));
-          b1 = fadd(b1, fmul(d, ucol[1][l]));
+          a = add2(a, mul2(pk2(dxr[l], dxr[l]), pair_load2(row + 2 * l), nz));
+          b = add2(b, mul2(pk2(d, d), uc[l], nz));
         }
-        float uxi[NC] = {a0, a1}, ueta[NC] = {b0, b1}, upt[NC] = {ucol[0][j], ucol[1][j]};
+        const float2 av = upk2(a), bv = upk2(b);
+        float uxi[NC] = {av.x, av.y}, ueta[NC] = {bv.x, bv.y}, upt[NC] = {ucol[0][j], ucol[1][j]};
         float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f};
         point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + 16, ax + 32, ax + 48,
                                     w2c[j]);
@@ -531,19 +562,19 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     for (int j = 0; j < NG; ++j) {
       float s[NC];
       if constexpr (PAIR) {
+        const float nzs = c_neg_zero;
+        const f2x nz = pk2(nzs, nzs);
         const float* row = frow + ridx(0, j, 0);
-        float acc0 = 0.0f, acc1 = 0.0f;
+        f2x acc = 0ull;  // (+0, +0)
 #pragma unroll
         for (int l = 0; l < NG; ++l) {
-          const float2 r = pair_load(row + 2 * l);
           const float d = cbasis(NG, 0, l * NG + j);
-          acc0 = fadd(acc0, fmul(dxc[l], r.x));
-          acc0 = fadd(acc0, fmul(d, fe[0][l]));
-          acc1 = fadd(acc1, fmul(dxc[l], r.y));
-          acc1 = fadd(acc1, fmul(d, fe[1][l]));
+          acc = add2(acc, mul2(pk2(dxc[l], dxc[l]), pair_load2(row + 2 * l), nz));
+          acc = add2(acc, mul2(pk2(d, d), pk2(fe[0][l], fe[1][l]), nz));
         }
-        s[0] = acc0;
-        s[1] = acc1;
+        const float2 sv = upk2(acc);
+        s[0] = sv.x;
+        s[1] = sv.y;
       } else {
 #pragma unroll
         for (int c = 0; c < NC; ++c) {

@@ -25,6 +25,8 @@ void INSEM_CAT(set_constant_basis_ng, INSEM_NG)(const float* D, const float* Dj,
     for (int q = 0; q < n; ++q) buf[q] = parts[which][q];
     CUDA_CHECK(cudaMemcpyToSymbol(c_basis, buf, sizeof(buf), sizeof(float) * 81 * (3 * (INSEM_NG - 2) + which)));
   }
+  const float neg_zero = -0.0f;
+  CUDA_CHECK(cudaMemcpyToSymbol(c_neg_zero, &neg_zero, sizeof(float)));
 }
 
 int INSEM_CAT(tile_elements_ng, INSEM_NG)() { return TileCfg<INSEM_NG>::TE; }
