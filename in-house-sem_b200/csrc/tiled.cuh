@@ -834,20 +834,51 @@ __device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev
   double kin = 0.0, pot = 0.0;
   if (h < hd.n) {
     const int32_t g = td.n_complete + h;
-    float f[NC], a[NC];
-    const int32_t b = hd.off[h], e = hd.off[h + 1];
+    // the point's own values first, all loads in flight together (the
+    // stores below may alias them for the compiler)
+    float uc[NC], vc[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
-      float s = 0.0f;
-      for (int32_t q = b; q < e; ++q) {
-        const float v = td.hbuf[static_cast<size_t>(c) * td.n_hbuf + hd.pos[q]];
-        s = fadd(s, hd.w ? fmul(hd.w[q], v) : v);
-      }
-      f[c] = s;
-      if (energy) pot = dadd(pot, dmul(static_cast<double>(td.u_cur[static_cast<size_t>(c) * td.ng + g]),
-                                       static_cast<double>(s)));
+      uc[c] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
+      vc[c] = td.v[static_cast<size_t>(c) * td.ng + g];
     }
+    const float im = td.inv_mass[g];
     const int32_t sp = hd.spec[h];
+    float f[NC], a[NC];
+    const int32_t b = hd.off[h], e = hd.off[h + 1];
+    constexpr int K = 4;  // contributions gathered at once (conforming 2D points have at most 4)
+    if (e - b <= K) {
+      int32_t pq[K];
+#pragma unroll
+      for (int q = 0; q < K; ++q) pq[q] = b + q < e ? hd.pos[b + q] : 0;
+      float vq[NC][K];
+#pragma unroll
+      for (int q = 0; q < K; ++q)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) vq[c][q] = b + q < e ? td.hbuf[static_cast<size_t>(c) * td.n_hbuf + pq[q]] : 0.0f;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        float s = 0.0f;
+#pragma unroll
+        for (int q = 0; q < K; ++q)
+          if (b + q < e) s = fadd(s, hd.w ? fmul(hd.w[b + q], vq[c][q]) : vq[c][q]);
+        f[c] = s;
+      }
+    } else {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        float s = 0.0f;
+        for (int32_t q = b; q < e; ++q) {
+          const float v = td.hbuf[static_cast<size_t>(c) * td.n_hbuf + hd.pos[q]];
+          s = fadd(s, hd.w ? fmul(hd.w[q], v) : v);
+        }
+        f[c] = s;
+      }
+    }
+    if (energy) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) pot = dadd(pot, dmul(static_cast<double>(uc[c]), static_cast<double>(f[c])));
+    }
     int32_t ai = -1;
     uint8_t zmask = 0;
     if (sp >= 0) {
@@ -879,7 +910,6 @@ __device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev
       ai = hd.abs_idx[sp];
       zmask = hd.zero[sp];
     }
-    const float im = td.inv_mass[g];
 #pragma unroll
     for (int c = 0; c < NC; ++c) a[c] = fmul(f[c], im);
     if (ai >= 0) {
@@ -891,8 +921,7 @@ __device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev
         rhs[r] = static_cast<double>(f[r]);
 #pragma unroll
         for (int s2 = 0; s2 < NC; ++s2) {
-          rhs[r] = dsub(rhs[r], dmul(static_cast<double>(cc[r * NC + s2]),
-                                     static_cast<double>(td.v[static_cast<size_t>(s2) * td.ng + g])));
+          rhs[r] = dsub(rhs[r], dmul(static_cast<double>(cc[r * NC + s2]), static_cast<double>(vc[s2])));
           A[r * NC + s2] = dadd(dmul(h_damp, static_cast<double>(cc[r * NC + s2])), r == s2 ? mass : 0.0);
         }
       }
@@ -905,8 +934,7 @@ __device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev
       if (zmask & (1u << c)) a[c] = 0.0f;
       const size_t gi = static_cast<size_t>(c) * td.ng + g;
       float u_out, v_state, v_n;
-      const float u = td.u_cur[gi];
-      complete_point(mode, sc, u, td.v[gi], a[c], u_out, v_state, v_n);
+      complete_point(mode, sc, uc[c], vc[c], a[c], u_out, v_state, v_n);
       td.u_nxt[gi] = u_out;
       td.v[gi] = v_state;
       td.a[gi] = a[c];
