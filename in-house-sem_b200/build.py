@@ -26,7 +26,7 @@ CASES_LIB = PKG / "lib" / "libinsem_cases.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
-    "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-relaxed-constexpr",
+    "-O3", "-lineinfo", "-std=c++17", "-fmad=false", "--expt-relaxed-constexpr", "--default-stream", "per-thread",
     "-Xcompiler", "-fPIC,-O3", "-I", str(REPO / "include"),
 ]
 

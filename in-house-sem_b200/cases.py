@@ -401,6 +401,25 @@ def build_from_arrays(model: Model, arrays: Dict[str, np.ndarray], device: int =
     return prob
 
 
+def build_solver_from_arrays(model: Model, arrays: Dict[str, np.ndarray], device: int = 0, **solver_kwargs):
+    """``build_from_arrays`` and ``Solver`` in one device construction: the
+    solver estimates the stable time step from the arrays it uploads and
+    applies the model's time settings (solver.cpp:131-144).  Same problem and
+    solver as the two-step route, with one upload instead of two.  Returns
+    (problem, solver)."""
+    from .solver import Solver
+
+    arrays = dict(arrays)
+    arrays["problem.dt"] = np.asarray(1.0)
+    arrays["problem.n_steps"] = np.asarray(0)
+    arrays["problem.stable_dt"] = np.asarray(0.0)
+    prob = ProblemData.from_npz(arrays)
+    s = Solver(prob, device=device, time=(model.dt if model.dt > 0.0 else 0.0, model.safety,
+                                          max(int(model.n_steps), 0), max(float(model.duration), 0.0)),
+               **solver_kwargs)
+    return prob, s
+
+
 # --------------------------------------------------------------- workloads
 MUD = Material.acoustic(1500.0, 1000.0)
 STEEL = Material.elastic(5900.0, 3200.0, 7850.0)

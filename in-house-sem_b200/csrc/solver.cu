@@ -86,7 +86,17 @@ void DeviceDomainData::alloc_fields() {
   fields_ready = true;
 }
 
-Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool setup_only) {
+void DeviceDomainData::free_fields() {
+  u.resize(0);
+  v.resize(0);
+  a.resize(0);
+  f.resize(0);
+  f_local.resize(0);
+  fields_ready = false;
+}
+
+Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool setup_only,
+               const insem_cuda_time* time) {
   if (opt) opts = *opt;
   else {
     opts = insem_cuda_options{};
@@ -103,7 +113,7 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
   INSEM_REQUIRE(p.n_domains >= 1 && p.n_domains <= 2, INSEM_CUDA_ERR_INVALID, "a problem has 1 or 2 domains");
   INSEM_REQUIRE(p.record_every >= 1, INSEM_CUDA_ERR_INVALID, "record_every must be >= 1");
   INSEM_REQUIRE(p.energy_every >= 0, INSEM_CUDA_ERR_INVALID, "energy_every must be >= 0");
-  INSEM_REQUIRE((setup_only || p.dt > 0.0) && p.n_steps >= 0, INSEM_CUDA_ERR_INVALID,
+  INSEM_REQUIRE((setup_only || time || p.dt > 0.0) && (time || p.n_steps >= 0), INSEM_CUDA_ERR_INVALID,
                 "dt must be positive and n_steps >= 0");
   dt = p.dt;
   n_steps = p.n_steps;
@@ -123,11 +133,30 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
   INSEM_REQUIRE(p.n_domains == 1 || (solid >= 0 && fluid >= 0), INSEM_CUDA_ERR_INVALID,
                 "two domains must be one acoustic and one elastic");
   build_coupling(p.coupling);
-  build_sources(p);
-  build_receivers(p);
   st = static_cast<StepState*>(device_alloc(sizeof(StepState)));
   CUDA_CHECK(cudaMemset(st, 0, sizeof(StepState)));
   partial.resize(static_cast<std::size_t>(kReduceBlocks) * 4);
+  if (time) {
+    // Solver::Solver (solver.cpp:131-144)
+    stable_dt_estimate = stable_dt();
+    if (time->dt > 0.0) {
+      INSEM_REQUIRE(time->dt <= stable_dt_estimate, INSEM_CUDA_ERR_INVALID,
+                    "time step " + std::to_string(time->dt) + " s exceeds the estimated stability limit " +
+                        std::to_string(stable_dt_estimate) + " s");
+      dt = time->dt;
+    } else {
+      INSEM_REQUIRE(time->safety > 0.0 && time->safety <= 1.0, INSEM_CUDA_ERR_INVALID,
+                    "time step safety factor must be in (0, 1]");
+      dt = time->safety * stable_dt_estimate;
+    }
+    if (time->n_steps > 0) n_steps = time->n_steps;
+    else if (time->duration > 0.0) n_steps = static_cast<int32_t>(std::ceil(time->duration / dt - 1e-9));
+    else n_steps = 0;
+    // the power iteration's two-pass fields; the path chosen below allocates what it uses
+    for (auto& d : domains) d.free_fields();
+  }
+  build_sources(p);
+  build_receivers(p);
   const int32_t n_energy = energy_every > 0 ? n_steps / energy_every + 1 : 0;
   energy.resize(static_cast<std::size_t>(std::max(n_energy, 1)) * 3);
   energy.zero();
@@ -401,6 +430,31 @@ double Solver::reduce_partials() {
   return s;
 }
 
+void Solver::replay(int n, const std::function<void()>& body) {
+  if (n <= 0) return;
+  cudaGraph_t g = nullptr;
+  CUDA_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+  try {
+    body();
+  } catch (...) {
+    // leave capture mode before the error propagates
+    if (cudaStreamEndCapture(stream, &g) == cudaSuccess && g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    throw;
+  }
+  CUDA_CHECK(cudaStreamEndCapture(stream, &g));
+  cudaGraphExec_t ge = nullptr;
+  const cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  CUDA_CHECK(e);
+  cudaError_t le = cudaSuccess;
+  for (int i = 0; i < n && le == cudaSuccess; ++i) le = cudaGraphLaunch(ge, stream);
+  const cudaError_t se = cudaStreamSynchronize(stream);
+  cudaGraphExecDestroy(ge);
+  CUDA_CHECK(le);
+  CUDA_CHECK(se);
+}
+
 // estimate_stable_dt (solver.cpp:583-619): 100 power iterations per domain
 // with x ~ U(-1, 1) from mt19937(12345), Rayleigh quotients in double.
 double Solver::stable_dt() {
@@ -421,7 +475,7 @@ double Solver::stable_dt() {
     DeviceBuffer<float> dx(n);
     CUDA_CHECK(cudaMemcpyAsync(dx.get(), x.data(), n * sizeof(float), cudaMemcpyHostToDevice, stream));
     CUDA_CHECK(cudaMemsetAsync(pw.get() + kPwDone, 0, sizeof(double), stream));
-    for (int it = 0; it < 100; ++it) {
+    replay(100, [&] {
       zero_constrained(d, dx.get());
       internal_forces(d, dx.get(), d.f.get());
       dot_partial_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(dx.get(), d.f.get(), n, st, 0, 1,
@@ -440,7 +494,7 @@ double Solver::stable_dt() {
       CUDA_LAUNCH_CHECK();
       scale_dev_kernel<<<grid_for(n), 256, 0, stream>>>(dx.get(), dx.get(), n, pw.get());
       CUDA_LAUNCH_CHECK();
-    }
+    });
     d.f.zero(stream);
     // dx is released below: its last kernels must have run
     CUDA_CHECK(cudaStreamSynchronize(stream));
@@ -479,7 +533,8 @@ void Solver::coupled_lambda_max(std::mt19937& rng, double* pw) {
     sum_partials_kernel<<<1, kReduceBlocks, 0, stream>>>(partial.get(), kReduceBlocks, 1.0, pw, slot);
     CUDA_LAUNCH_CHECK();
   };
-  for (int it = 0; it < 120; ++it) {
+  // iterations 0..59 and 60..119 differ only in coupled_step_kernel's test it >= 60
+  auto iteration = [&](int it) {
     zero_constrained(sd, sd.u.get());
     zero_constrained(fd, fd.u.get());
     mass_norm(sd, sd.u.get(), kPwA);
@@ -506,7 +561,9 @@ void Solver::coupled_lambda_max(std::mt19937& rng, double* pw) {
       scale_dev_kernel<<<grid_for(n), 256, 0, stream>>>(d->a.get(), d->u.get(), n, pw);
       CUDA_LAUNCH_CHECK();
     }
-  }
+  };
+  replay(60, [&] { iteration(0); });
+  replay(60, [&] { iteration(60); });
   for (DeviceDomainData* d : {&sd, &fd}) {
     d->u.zero(stream);
     d->a.zero(stream);
@@ -1072,6 +1129,18 @@ int insem_cuda_solver_create(const insem_cuda_problem* problem, const insem_cuda
     *out = h.release();
   });
 }
+
+int insem_cuda_solver_create_timed(const insem_cuda_problem* problem, const insem_cuda_time* time,
+                                   const insem_cuda_options* options, insem_cuda_solver** out) {
+  return guarded([&] {
+    INSEM_REQUIRE(problem && time && out, INSEM_CUDA_ERR_INVALID, "null argument");
+    auto h = std::make_unique<insem_cuda_solver>();
+    h->s = std::make_unique<Solver>(*problem, options, false, time);
+    *out = h.release();
+  });
+}
+
+double insem_cuda_solver_stable_dt(const insem_cuda_solver* h) { return h ? h->s->stable_dt_estimate : 0.0; }
 
 void insem_cuda_solver_destroy(insem_cuda_solver* h) { delete h; }
 

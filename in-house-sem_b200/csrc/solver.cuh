@@ -1,6 +1,8 @@
 // Device-resident solver state (the twin of solver::Solver).
 #pragma once
 
+#include <functional>
+
 #include <memory>
 #include <random>
 #include <vector>
@@ -27,6 +29,7 @@ struct DeviceDomainData {
   DeviceBuffer<float> u, v, a, f, f_local;  // two-pass path only (alloc_fields)
   bool fields_ready = false;
   void alloc_fields();
+  void free_fields();
 
   void upload(const insem_cuda_domain& d, const insem_cuda_basis& basis);
 };
@@ -47,7 +50,10 @@ struct BatchTables;
 class Solver {
  public:
   // setup_only: dt may be 0 (the problem is used to estimate the stable time step).
-  Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool setup_only = false);
+  // time: dt and n_steps come from the stable time step estimated here
+  // (solver.cpp:131-144) instead of from the problem.
+  Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool setup_only = false,
+         const insem_cuda_time* time = nullptr);
   ~Solver();
   Solver(const Solver&) = delete;
   Solver& operator=(const Solver&) = delete;
@@ -74,6 +80,7 @@ class Solver {
   int device = 0;
   int ngll = 0;
   double dt = 0.0;
+  double stable_dt_estimate = 0.0;  // set by the timed constructor
   int32_t n_steps = 0, step = 0, record_every = 1, energy_every = 0;
   bool initialized = false;
   double last_ms = 0.0;
@@ -97,6 +104,9 @@ class Solver {
   void zero_constrained(DeviceDomainData& d, float* x);
   void coupling_forces(int di);
   void coupled_lambda_max(std::mt19937& rng, double* pw);
+  // Runs `body` (launches on `stream` only) n times: captured once as a CUDA
+  // graph and replayed; returns after the stream has drained.
+  void replay(int n, const std::function<void()>& body);
 
   DeviceBasis basis;
   int solid = -1, fluid = -1;

@@ -90,6 +90,11 @@ class Problem(C.Structure):
                 ("n_steps", C.c_int32), ("record_every", C.c_int32), ("energy_every", C.c_int32)]
 
 
+class Time(C.Structure):
+    """insem_cuda_time: the reference's TimeConfig (dt, safety, n_steps, duration)."""
+    _fields_ = [("dt", C.c_double), ("safety", C.c_double), ("n_steps", C.c_int32), ("duration", C.c_double)]
+
+
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("use_graphs", C.c_int32), ("path", C.c_int32),
                 ("tile_elements", C.c_int32), ("check_finite", C.c_int32)]
@@ -119,6 +124,9 @@ def lib() -> C.CDLL:
             "insem_cuda_gather": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
             "insem_cuda_assemble": (C.c_int, [vp, C.c_int32, vp, vp, vp]),
             "insem_cuda_solver_create": (C.c_int, [C.POINTER(Problem), C.POINTER(Options), C.POINTER(vp)]),
+            "insem_cuda_solver_create_timed": (C.c_int, [C.POINTER(Problem), C.POINTER(Time), C.POINTER(Options),
+                                                         C.POINTER(vp)]),
+            "insem_cuda_solver_stable_dt": (C.c_double, [vp]),
             "insem_cuda_solver_destroy": (None, [vp]),
             "insem_cuda_solver_set_state": (C.c_int, [vp, C.c_int32, f64p, f64p]),
             "insem_cuda_solver_advance": (C.c_int, [vp, C.c_int32]),

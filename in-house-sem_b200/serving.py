@@ -182,8 +182,7 @@ def _stage_host(req: Request):
 def _stage_device(model, arrays, device: int, use_graphs: bool, prepare: bool):
     """Stage B (device, worker thread): dt from the power iteration, the solver
     (and, for the batched server, its initial step and predictor)."""
-    prob = K.build_from_arrays(model, arrays, device=device)
-    s = Solver(prob, device=device, use_graphs=use_graphs)
+    prob, s = K.build_solver_from_arrays(model, arrays, device=device, use_graphs=use_graphs)
     if prepare:
         s.prepare_for_batch()
     return prob, s

@@ -17,12 +17,23 @@ from .problem import ProblemData
 
 class Solver:
     def __init__(self, problem: ProblemData, device: int = 0, use_graphs: bool = True, path: int = 0,
-                 tile_elements: int = 0, check_finite: bool = True):
+                 tile_elements: int = 0, check_finite: bool = True, time: Optional[Tuple[float, float, int, float]] = None):
+        """``time`` = (dt, safety, n_steps, duration), the reference's time
+        settings: the solver then estimates the stable time step on the device
+        and derives dt and n_steps as the reference Solver constructor does
+        (solver.cpp:131-144); ``problem`` gets dt, n_steps and stable_dt."""
         self.problem = problem
         self._packed = problem.to_c()
         opts = N.Options(device, int(use_graphs), path, tile_elements, int(check_finite))
         h = C.c_void_p()
-        N.check(N.lib().insem_cuda_solver_create(self._packed.ref(), C.byref(opts), C.byref(h)))
+        if time is None:
+            N.check(N.lib().insem_cuda_solver_create(self._packed.ref(), C.byref(opts), C.byref(h)))
+        else:
+            t = N.Time(float(time[0]), float(time[1]), int(time[2]), float(time[3]))
+            N.check(N.lib().insem_cuda_solver_create_timed(self._packed.ref(), C.byref(t), C.byref(opts), C.byref(h)))
+            problem.dt = float(N.lib().insem_cuda_solver_dt(h))
+            problem.n_steps = int(N.lib().insem_cuda_solver_n_steps(h))
+            problem.stable_dt = float(N.lib().insem_cuda_solver_stable_dt(h))
         self._h = h
         self._traces = problem.trace_list()
 

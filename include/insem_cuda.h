@@ -16,6 +16,8 @@
  *   insem_cuda_solver_*    solver::Solver (cpp/include/insem/solver/solver.hpp:91-228):
  *                          advance / run / set_state / traces / energy / state
  *   insem_cuda_stable_dt   Solver::estimate_stable_dt + coupled_lambda_max
+ *   insem_cuda_solver_create_timed  Solver::Solver's stable-dt and dt / n_steps
+ *                          rule (solver.cpp:131-144)
  *                          (cpp/src/solver/solver.cpp:583-667), FP64 reductions
  *   insem_cuda_batch_*     many independent solves advanced by shared launches
  *                          (the serving loop admits and retires solves through it)
@@ -248,6 +250,28 @@ typedef struct insem_cuda_solver insem_cuda_solver;
 /* Uploads a problem; fields start at zero.  `options` may be NULL. */
 int insem_cuda_solver_create(const insem_cuda_problem* problem, const insem_cuda_options* options,
                              insem_cuda_solver** out);
+
+/* Time settings (TimeConfig, cpp/include/insem/sim/description.hpp:128-135). */
+typedef struct insem_cuda_time {
+  double dt;        /* > 0: this step (it must not exceed the stability limit); 0: safety x stable dt */
+  double safety;    /* share of the stability limit used when dt = 0, in (0, 1] */
+  int32_t n_steps;  /* > 0: this many steps; 0: ceil(duration / dt - 1e-9) */
+  double duration;  /* simulated seconds, used when n_steps = 0 */
+} insem_cuda_time;
+
+/* The reference Solver constructor's time handling (solver.cpp:131-144): the
+ * problem's dt and n_steps are ignored; the solver estimates the stable time
+ * step on the device from the arrays it has just uploaded (as
+ * insem_cuda_stable_dt does) and derives dt and n_steps from `time`.  Same
+ * result as insem_cuda_stable_dt followed by insem_cuda_solver_create with
+ * the derived dt and n_steps, with one upload of the problem instead of two.
+ * A dt above the stability limit or a safety outside (0, 1] is
+ * INSEM_CUDA_ERR_INVALID, as in the reference. */
+int insem_cuda_solver_create_timed(const insem_cuda_problem* problem, const insem_cuda_time* time,
+                                   const insem_cuda_options* options, insem_cuda_solver** out);
+/* The stable time step estimated by insem_cuda_solver_create_timed (0 for a
+ * solver made by insem_cuda_solver_create). */
+double insem_cuda_solver_stable_dt(const insem_cuda_solver* h);
 void insem_cuda_solver_destroy(insem_cuda_solver* h);
 /* Initial conditions of one medium ([ncomp][n_global], host doubles), before
  * the first step only (Solver::set_state, solver.cpp:764-778). */

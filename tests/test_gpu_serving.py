@@ -65,3 +65,37 @@ def test_plain_server_runs_the_same_stream(pkg):
     recs = S.serve_plain(stream, keep_traces=True)
     for r in stream:
         assert np.array_equal(recs[r.rid].traces, _solo_traces(r))
+
+
+def test_timed_constructor_matches_two_step_route(pkg):
+    """One device construction with the stable time step estimated inside
+    (solver.cpp:131-144) gives the dt, step count and traces of
+    stable-dt estimate + construction, bit for bit; a dt above the limit is
+    rejected as in the reference."""
+    from insem_b200 import Solver, cases as K, native as N, serving as S
+
+    stream = _small_stream()
+    seen = set()
+    for r in stream:
+        if r.kind in seen:
+            continue
+        seen.add(r.kind)
+        model, arrays, _ = S.setup_request(r)
+        prob_a = K.build_from_arrays(model, arrays)
+        with Solver(prob_a) as a:
+            a.run()
+            ta = np.concatenate([a.trace_by_index(t) for t in range(len(prob_a.trace_list()))], axis=1)
+        prob_b, b = K.build_solver_from_arrays(model, arrays)
+        with b:
+            assert prob_b.stable_dt == prob_a.stable_dt, r.kind
+            assert b.dt == prob_a.dt and b.n_steps == prob_a.n_steps, r.kind
+            b.run()
+            tb = np.concatenate([b.trace_by_index(t) for t in range(len(prob_b.trace_list()))], axis=1)
+        assert np.array_equal(ta, tb), r.kind
+    assert len(seen) >= 3
+    model, arrays, _ = S.setup_request(stream[0])
+    sdt = K.build_from_arrays(model, arrays).stable_dt
+    model.dt = 2.0 * sdt
+    with pytest.raises(N.InsemError) as e:
+        K.build_solver_from_arrays(model, arrays)
+    assert e.value.code == N.ERR_INVALID and "stability limit" in str(e.value)
