@@ -319,10 +319,22 @@ def build_config4(args, device):
     from insem_b200 import autotune
     from insem_b200 import cases as K
 
-    probs = []
+    from concurrent.futures import ThreadPoolExecutor
+
+    probs, chunk = [], []
+
+    def flush():
+        with ThreadPoolExecutor(max_workers=len(chunk)) as ex:
+            probs.extend(ex.map(lambda c: (c[0], K.build_from_arrays(c[1], c[2], device=device)), chunk))
+        chunk.clear()
+
+    # stable-dt estimates in threads, 16 models' host arrays held at a time
     for p, model, arrays, ne, geo in K.config4(args.models, 4):
-        probs.append((p, K.build_from_arrays(model, arrays, device=device)))
-        del arrays
+        chunk.append((p, model, arrays))
+        if len(chunk) == 16:
+            flush()
+    if chunk:
+        flush()
     t0 = time.perf_counter()
     table = None if args.no_autotune else autotune.tune_batched([q for _, q in probs], device=device)
     tune_s = time.perf_counter() - t0

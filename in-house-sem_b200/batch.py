@@ -2,7 +2,7 @@
 
 Every batched step is one CUDA graph with a fixed number of launches,
 whatever the number of problems:
-- persistent tile kernels per tile class pull work from a device queue;
+- one tile kernel per tile class, whose CTAs pull tiles from a device queue;
 - then the point-wise kernels of all problems run.
 
 Each problem keeps its own time step and step count. A problem's results in

@@ -311,7 +311,9 @@ void Batch::rebuild() {
     a.L = d.L;
     a.smem = d.L.total;
     const int per_sm = std::max(1, tile_batch(c.ngll, a, false));
-    d.grid = std::max(1, std::min(d.n_items, per_sm * n_sms));
+    // one CTA per item (the call above also sets the kernel's shared memory size)
+    (void)per_sm;
+    d.grid = std::max(1, d.n_items);
     dclasses.push_back(std::move(d));
   }
   if (queues.size() != std::max<std::size_t>(dclasses.size(), 1)) queues.resize(std::max<std::size_t>(dclasses.size(), 1));

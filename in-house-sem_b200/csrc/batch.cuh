@@ -6,8 +6,8 @@
 // the number of solves:
 //   begin (step counters, buffer parities, modes; tile queues reset)
 //   constrained-slot gathers of every solve
-//   one persistent tile launch per tile class (ngll, kind, medium, order):
-//     CTAs pull (segment, tile) items from a device work queue
+//   one tile launch per tile class (ngll, kind, medium, order): each CTA
+//     pulls a (segment, tile) item from a device work queue
 //   halo points of every solve (elastic classes, then acoustic: the fluid's
 //     coupling term reads the solid's new acceleration)
 //   receivers (particle velocity, then recording) and energy of every solve

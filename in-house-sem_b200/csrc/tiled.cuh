@@ -162,8 +162,7 @@ __device__ __forceinline__ float cbasis(int ng, int which, int idx) { return c_b
 // Two mbarriers per CTA track the tile's bulk copies (cp.async.bulk, the
 // non-tensor TMA path), one for the copies at the start of a tile and one
 // for the late copies: thread 0 announces the byte count and issues the
-// copies; every thread waits on the barrier's current phase (the persistent
-// kernel's tiles alternate the phase).
+// copies; every thread waits on the barrier's phase 0 (one tile per CTA).
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
@@ -735,9 +734,13 @@ struct TileSeg {
   int32_t tile0;        // the block's first tile in the domain's tile table
 };
 
-// Persistent CTAs take work items (segment, tile within the block) from a
-// device queue: `queue` is zeroed by the step's first kernel.  One shared
-// memory layout serves the class (sized for its largest tile).
+// Work items (segment, tile within the block) come from a device queue:
+// `queue` is zeroed by the step's first kernel.  The grid has one CTA per
+// item.  A CTA claims items until it holds one of a running solve (items of
+// finished solves are skipped), finishes that tile and exits.  (CTAs that
+// loop over items measured slower: the loop keeps about 40 more registers
+// per thread live, which costs resident CTAs per SM.)  One shared memory
+// layout serves the class (sized for its largest tile).
 template <int NG, int KIND, bool EL, int M>
 static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
     tile_batch_kernel(const TileSeg* __restrict__ segs, const int2* __restrict__ items, int32_t n_items,
@@ -751,8 +754,6 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
   }
-  __syncthreads();
-  uint32_t phase = 0;
   for (;;) {
     if (threadIdx.x == 0) {
       const int32_t w = atomicAdd(queue, 1);
@@ -764,7 +765,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
       }
     }
     __syncthreads();
-    if (s_item >= n_items) break;
+    if (s_item >= n_items) return;
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(segs + s_segi);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&s_seg);
@@ -780,14 +781,11 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
       }
     }
     __syncthreads();
-    if (s_idle) continue;  // a finished solve: no copies issued, the barrier phase is unchanged
-    const int32_t local = s_tile;
-    const bool ok = tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial,
-                                                    s_seg.tile0 + local, L, smem_raw, bar, phase);
-    if (!ok) break;
-    phase ^= 1u;
-    __syncthreads();  // the next item's copies overwrite shared memory
+    if (!s_idle) break;
+    __syncthreads();  // the next claim rewrites the item and the segment
   }
+  tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial, s_seg.tile0 + s_tile, L,
+                                  smem_raw, bar, 0u);
 }
 
 // ------------------------------------------------------------ halo kernel

@@ -89,8 +89,8 @@ int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp);
 void set_constant_basis(int ngll, const std::vector<float>& D, const std::vector<float>& Dj,
                         const std::vector<float>& w2);
 
-// Batched tile launches: one persistent launch per tile class (ngll, kind,
-// medium, order) over the work items of many solves.
+// Batched tile launches: one launch per tile class (ngll, kind, medium,
+// order) over the work items of many solves, one CTA per item.
 struct TileBatchLaunch {
   int kind = 0, m = 0;
   bool elastic = false;

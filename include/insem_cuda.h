@@ -355,8 +355,8 @@ int insem_cuda_stable_dt(const insem_cuda_problem* problem, int32_t device, doub
 /* ---------------------------------------------------------- batched solves */
 /* Many independent solves (models, shots) of any ngll, geometry kind, medium
  * and azimuthal order, advanced together: every batched step is one CUDA
- * graph of a fixed number of launches (persistent tile launches per tile
- * class fed by a device work queue, then the point-wise kernels of all
+ * graph of a fixed number of launches (one tile launch per tile class, its
+ * CTAs fed by a device work queue, then the point-wise kernels of all
  * solves).  Each solve keeps its own time step and step count and gets the
  * results it gets alone, bit for bit.  The reference has no batch API; its
  * nearest form is one Simulation per thread (bindings.cpp:336-337).
