@@ -328,10 +328,10 @@ def build_config4(args, device):
             probs.extend(ex.map(lambda c: (c[0], K.build_from_arrays(c[1], c[2], device=device)), chunk))
         chunk.clear()
 
-    # stable-dt estimates in threads, 16 models' host arrays held at a time
-    for p, model, arrays, ne, geo in K.config4(args.models, 4):
+    # stable-dt estimates in threads, one chunk of models' host arrays held at a time
+    for p, model, arrays, ne, geo in K.config4(args.models, workers=max(1, min(4, args.setup_threads))):
         chunk.append((p, model, arrays))
-        if len(chunk) == 16:
+        if len(chunk) == max(1, args.setup_threads):
             flush()
     if chunk:
         flush()
@@ -520,10 +520,12 @@ def main():
     ap.add_argument("--config3-steps", type=int, default=200, help="steps of the config3 sub-run")
     ap.add_argument("--no-config3", action="store_true", help="skip the config3 sub-run")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload: keep the default tile sizes")
+    ap.add_argument("--setup-threads", type=int, default=16,
+                    help="batched workload: host threads building the models and their stable time steps")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-window", type=float, default=4.0, help="serving: seconds of arrivals")
-    ap.add_argument("--serve-scale", type=float, default=0.05, help="serving: factor on the simulated durations")
+    ap.add_argument("--serve-scale", type=float, default=0.25, help="serving: factor on the simulated durations")
     ap.add_argument("--serve-chunk", type=int, default=64, help="serving: batched steps between admissions")
     ap.add_argument("--serve-plain-fraction", type=float, default=0.25,
                     help="serving: share of the stream (from its start) also served by the plain path")
