@@ -38,7 +38,7 @@ struct DeviceBasis {
 // elements taken in `order` (block-local positions): metric Rect 4 / Affine 8
 // floats per element, per-point arrays CS = npe rounded up to 4 per element,
 // per-point metric [element][component][CS] (transposed from the reference's
-// [element][point][5]).
+// [element][point][5]; axisymmetric blocks keep the first 4 components).
 struct PackedBlock {
   std::vector<float> metric, coef0, coef1, wr, hoop, r;
   std::vector<uint8_t> axial;
@@ -69,8 +69,9 @@ inline PackedBlock pack_block(const insem_cuda_block& b, int npe, int medium, co
       const int src = b.kind == INSEM_RECT ? 3 : 5;
       for (int k = 0; k < src; ++k) pk.metric[q * ms + k] = b.metric[o * src + k];
     } else {
+      const int rows = axi ? 4 : 5;
       for (int k = 0; k < npe; ++k)
-        for (int c = 0; c < 5; ++c) pk.metric[(q * 5 + c) * cs + k] = b.metric[(o * npe + k) * 5 + c];
+        for (int c = 0; c < rows; ++c) pk.metric[(q * rows + c) * cs + k] = b.metric[(o * npe + k) * 5 + c];
     }
     for (int k = 0; k < npe; ++k) {
       pk.coef0[q * cs + k] = b.coef0[o * npe + k];

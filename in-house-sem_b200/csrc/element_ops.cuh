@@ -130,14 +130,16 @@ __device__ __forceinline__ void el_stress(float lambda, float mu, float ux_x, fl
 // element's data can be moved with bulk copies):
 //   per-point arrays: CS = npe rounded up to 4 floats per element (and per
 //                     metric component);
-//   metric: Rect 4 floats, Affine 8 floats, Curved / Axisym 5 * CS floats.
+//   metric: Rect 4 floats, Affine 8 floats, Curved 5 * CS floats (xi_x,
+//           xi_z, eta_x, eta_z, jac), Axisym 4 * CS (xi_r, xi_z, eta_r, eta_z:
+//           the axisymmetric fluxes use the Jacobian only through wr).
 template <int NPE>
 constexpr int point_stride() {
   return (NPE + 3) & ~3;
 }
 inline int point_stride_rt(int npe) { return (npe + 3) & ~3; }
 inline int metric_stride_rt(int kind, int npe) {
-  return kind == INSEM_RECT ? 4 : kind == INSEM_AFFINE ? 8 : 5 * point_stride_rt(npe);
+  return kind == INSEM_RECT ? 4 : kind == INSEM_AFFINE ? 8 : (kind == INSEM_AXISYM ? 4 : 5) * point_stride_rt(npe);
 }
 
 // Metric of block element b at point k in the device layout.
@@ -224,7 +226,7 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
     }
   } else {
     const size_t p = static_cast<size_t>(bb) * CS + kpt;
-    const float* mt = blk.metric + static_cast<size_t>(bb) * 5 * CS + kpt;
+    const float* mt = blk.metric + static_cast<size_t>(bb) * 4 * CS + kpt;
     const float xi_r = mt[0], xi_z = mt[CS], eta_r = mt[2 * CS], eta_z = mt[3 * CS];
     const bool axis_pt = axial && i == 0;
     if constexpr (ELASTIC && M == 0) {

@@ -218,7 +218,7 @@ struct TileLayout {
     TileLayout L{};
     const int npe = ng * ng;
     L.cs = (npe + 3) & ~3;
-    L.ms = kind == INSEM_RECT ? 4 : kind == INSEM_AFFINE ? 8 : 5 * L.cs;
+    L.ms = kind == INSEM_RECT ? 4 : kind == INSEM_AFFINE ? 8 : (kind == INSEM_AXISYM ? 4 : 5) * L.cs;
     L.row = (ng + 1) & ~1;
     L.tp_cap = tp_cap;
     L.nc_cap = nc_cap;
@@ -266,7 +266,7 @@ struct TileLayout {
     L.im = p + tf_b + v_b;
     if (!L.late) o += tf_b + v_b + im_b;
     L.ax = o;
-    if (axi) o = up16(o + 4u * te * 64);
+    if (axi) o = up16(o + 4u * te * 4 * ((ng + 3) & ~3));
     L.total = o;
     return L;
   }
@@ -343,7 +343,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   constexpr int CS = point_stride<NPE>();
   constexpr int ROW = Cfg::ROW;
   constexpr bool AXI = KIND == INSEM_AXISYM;
-  constexpr int MS = KIND == INSEM_RECT ? 4 : KIND == INSEM_AFFINE ? 8 : 5 * CS;
+  constexpr int MS = KIND == INSEM_RECT ? 4 : KIND == INSEM_AFFINE ? 8 : (AXI ? 4 : 5) * CS;
   float* s_metric = reinterpret_cast<float*>(smem_raw + L.metric);
   float* s_coef0 = reinterpret_cast<float*>(smem_raw + L.coef0);
   float* s_coef1 = reinterpret_cast<float*>(smem_raw + L.coef1);
@@ -357,7 +357,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   float* tf = reinterpret_cast<float*>(smem_raw + L.tf);   // [NC][tp_cap]
   float* su = reinterpret_cast<float*>(smem_raw + L.su);   // [TE][NC][NG][ROW] field rows, later staging
   float* sfx = reinterpret_cast<float*>(smem_raw + L.sfx); // [TE][NC][NG][ROW] f_xi rows
-  float* sax = reinterpret_cast<float*>(smem_raw + L.ax);  // [TE][4][16] axis terms
+  float* sax = reinterpret_cast<float*>(smem_raw + L.ax);  // [TE][4][AXS] axis terms
   const int tp_cap = L.tp_cap, nc_cap = L.nc_cap;
 
   const TileHdr th = td.tiles[tile];
@@ -427,7 +427,8 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   auto ridx = [](int c, int j, int l) { return PAIR ? j * 2 * NG + 2 * l + c : (c * NG + j) * ROW + l; };
   float* urow = su + el * ES;
   float* frow = sfx + el * ES;
-  float* ax = sax + el * 64;
+  constexpr int AXS = (NG + 3) & ~3;  // one axis-term array (gx0, gy0, gx1, gy1) of an element
+  float* ax = sax + el * 4 * AXS;
 
   // 2. element field rows (slots through their tile point or the constrained list)
   uint32_t dsc[NG];
@@ -495,8 +496,8 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
         const float2 av = upk2(a), bv = upk2(b);
         float uxi[NC] = {av.x, av.y}, ueta[NC] = {bv.x, bv.y}, upt[NC] = {ucol[0][j], ucol[1][j]};
         float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f};
-        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + 16, ax + 32, ax + 48,
-                                    w2c[j]);
+        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
+                                    ax + 3 * AXS, w2c[j]);
         fx[0][j] = fxp[0];
         fx[1][j] = fxp[1];
         fe[0][j] = fy[0];
@@ -528,8 +529,8 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
         float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
-        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + 16, ax + 32, ax + 48,
-                                    w2c[j]);
+        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
+                                    ax + 3 * AXS, w2c[j]);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
           fx[c][j] = fxp[c];
@@ -590,7 +591,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       const float drj[2] = {dir[0][j], dir[1][j]};
       float out[NC];
       point_divergence<NG, KIND, EL, M>(i, j, axial, s, drj, dxc[0], [](int q) { return cbasis(NG, 0, q); }, ax,
-                                        ax + 16, ax + 32, ax + 48, out);
+                                        ax + AXS, ax + 2 * AXS, ax + 3 * AXS, out);
 #pragma unroll
       for (int c = 0; c < NC; ++c) fo[c][j] = out[c];
     }

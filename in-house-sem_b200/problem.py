@@ -151,15 +151,16 @@ class ProblemData:
     def algorithmic_bytes_per_step(self) -> int:
         """Minimum HBM bytes of one step (fp32):
         sum_domains n_g (16 ncomp + 4) + sum_elements [4 npe + metric(kind) + coef],
-        metric Rect 12, Affine 20, Curved 20 npe, Axisym 32 npe; coef elastic 8 npe,
-        acoustic 4 npe."""
+        metric Rect 12, Affine 20, Curved 20 npe, Axisym 28 npe (xi_r, xi_z,
+        eta_r, eta_z, wr, hoop, r: the axisymmetric fluxes use the Jacobian only
+        through wr); coef elastic 8 npe, acoustic 4 npe."""
         npe = self.ngll * self.ngll
         total = 0
         for d in self.domains:
             total += d.n_global * (16 * d.ncomp + 4)
             coef = (8 if d.medium == N.ELASTIC else 4) * npe
             for b in d.blocks:
-                metric = {N.RECT: 12, N.AFFINE: 20, N.CURVED: 20 * npe, N.AXISYM: 32 * npe}[b.kind]
+                metric = {N.RECT: 12, N.AFFINE: 20, N.CURVED: 20 * npe, N.AXISYM: 28 * npe}[b.kind]
                 total += b.n_elements * (4 * npe + metric + coef)
         return int(total)
 
@@ -175,7 +176,7 @@ class ProblemData:
             halo += (d.n_global - nt) * per_point
             coef = (8 if d.medium == N.ELASTIC else 4) * npe
             for b in d.blocks:
-                metric = {N.RECT: 12, N.AFFINE: 20, N.CURVED: 20 * npe, N.AXISYM: 32 * npe}[b.kind]
+                metric = {N.RECT: 12, N.AFFINE: 20, N.CURVED: 20 * npe, N.AXISYM: 28 * npe}[b.kind]
                 tile += b.n_elements * (4 * npe + metric + coef)
         return int(tile), int(halo)
 
