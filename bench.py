@@ -13,7 +13,7 @@ receivers, 5 ms), built by the native setup.  A step is one batched step:
 one time step of every model (each with its own dt).
 
 value      device time (CUDA events) of K batched steps, every input resident
-           in HBM; a batched step touches ~15 GB, far more than L2.
+           in HBM; a batched step touches ~16 GB, far more than L2.
 plain      the same models with the plain one-solve-per-launch path (each
            solve's own step graph, solves one after another), device time.
 e2e        the same metric through the C ABI's streamed batched steps: every
@@ -243,11 +243,12 @@ def cpu_baseline_config4(warmup: int, steps: int, sample_models: int = 4) -> dic
 def run_reference(args, world, rank):
     if rank != 0:
         return
+    # exactly --steps timed steps after --warmup, each a bounded sample of the workload
     if args.workload == "config3":
-        base = cpu_baseline_config3(args.warmup, args.cpu_steps)
+        base = cpu_baseline_config3(args.warmup, args.steps)
         workload = f"config3 coupled 2D Cartesian, order 5, sample nx={REF_SAMPLE_NX}"
     else:
-        base = cpu_baseline_config4(max(1, min(args.warmup, 2)), args.cpu_steps)
+        base = cpu_baseline_config4(args.warmup, args.steps)
         workload = "config4 batched boreholes (reference: models in sequence, all host cores)"
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": METRIC, "n_gpus": args.gpus,
             "steps": base["steps"], "warmup": args.warmup, "ms_per_step": 1e3 * base["seconds"] / base["steps"],
