@@ -153,7 +153,7 @@ int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp) {
     const double halo = static_cast<double>(tp - nc) / tp;                 // points shared with other tiles
     const double overlap = ctas >= 3 ? 1.0 : ctas == 2 ? 0.9 : 0.6;       // copies of one tile under another's math
     const double lanes = static_cast<double>(te * ngll) / tile_threads(te, ngll);  // threads with an element column
-    const double score = ctas * te * (1.0 - 0.5 * halo) * overlap * (0.8 + 0.2 * lanes);
+    const double score = ctas * te * (1.0 - 0.5 * halo) * overlap * lanes;
     if (score > best + 1e-9) {
       best = score;
       best_te = te;
