@@ -31,6 +31,7 @@ from __future__ import annotations
 import time
 from collections import deque
 from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
 from dataclasses import dataclass
 from typing import Dict, List, Optional
 
@@ -259,13 +260,29 @@ class _Pipeline:
 
 
 # ------------------------------------------------------------------ servers
+# Tile sizes that autotune.tune_batched measured on a B200 for the borehole
+# tile classes (axisymmetric elastic, ngll 5-7, m = 0 and 1: the classes of
+# every borehole request), in autotune.save's format.  Other classes keep the
+# occupancy-based default.  Tile sizes change speed only, never results.
+DEFAULT_TILE_TABLE = Path(__file__).resolve().parent / "data" / "tile_table_b200.json"
+
+
+def _load_tiles(tile_table) -> None:
+    """Registers a saved tile table for the whole process (None: keep the current choices)."""
+    if tile_table:
+        from . import autotune
+
+        autotune.load(str(tile_table))
+
+
 class Server:
     """Continuous-batching server over one Batch on one device."""
 
     def __init__(self, device: int = 0, hbm_budget: Optional[int] = None, chunk_steps: int = 64,
-                 workers: Optional[int] = None, use_graphs: bool = True):
+                 workers: Optional[int] = None, use_graphs: bool = True, tile_table=DEFAULT_TILE_TABLE):
         import os
 
+        _load_tiles(tile_table)
         self.device = device
         free, _ = mem_info(device)
         self.budget = int(hbm_budget) if hbm_budget else int(0.8 * free)
@@ -316,11 +333,14 @@ class Server:
 
 
 def serve_plain(stream: List[Request], device: int = 0, workers: Optional[int] = None,
-                keep_traces: bool = False, hbm_budget: Optional[int] = None) -> Dict[int, Record]:
-    """The plain path on the same stream and the same setup pipeline. Requests
-    are solved one at a time in arrival order, each with its own step graphs."""
+                keep_traces: bool = False, hbm_budget: Optional[int] = None,
+                tile_table=DEFAULT_TILE_TABLE) -> Dict[int, Record]:
+    """The plain path on the same stream, the same setup pipeline and the same
+    tile sizes. Requests are solved one at a time in arrival order, each with
+    its own step graphs."""
     import os
 
+    _load_tiles(tile_table)
     recs = {r.rid: Record(r.rid, r.kind, r.arrival) for r in stream}
     free, _ = mem_info(device)
     pipe = _Pipeline(stream, recs, device, int(hbm_budget) if hbm_budget else int(0.8 * free),

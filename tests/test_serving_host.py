@@ -38,3 +38,23 @@ def test_request_models_set_up(pkg):
         assert ne > 0 and model.duration == r.spec["duration"]
         seen.add(r.kind)
     assert seen == set(S.KINDS)
+
+
+def test_shipped_tile_table_registers(pkg):
+    """The B200 tile table the servers load covers the borehole classes and
+    registers every entry (tile sizes change speed only, never results)."""
+    import json
+
+    from insem_b200 import autotune, native as N, serving as S
+
+    rows = json.loads(S.DEFAULT_TILE_TABLE.read_text())["tiles"]
+    keys = {tuple(r["class"]) for r in rows}
+    assert {(ng, N.AXISYM, N.ELASTIC, m, 3 if m else 2) for ng in (5, 6, 7) for m in (0, 1)} <= keys
+    before = {k: autotune.current(k) for k in keys}
+    try:
+        S._load_tiles(S.DEFAULT_TILE_TABLE)
+        for r in rows:
+            assert autotune.current(tuple(r["class"])) == min(r["te"], autotune.te_max(r["class"][0]))
+    finally:
+        for k, te in before.items():
+            autotune.register(k, te)
