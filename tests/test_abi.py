@@ -47,10 +47,11 @@ def test_struct_layout_matches_header(pkg):
 #include <stdio.h>
 #include "insem_cuda.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(insem_cuda_basis), sizeof(insem_cuda_block),
-         sizeof(insem_cuda_dofmap), sizeof(insem_cuda_domain), sizeof(insem_cuda_coupling), sizeof(insem_cuda_stf),
-         sizeof(insem_cuda_source), sizeof(insem_cuda_receiver), sizeof(insem_cuda_problem),
-         sizeof(insem_cuda_options), offsetof(insem_cuda_problem, dt));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(insem_cuda_basis),
+         sizeof(insem_cuda_block), sizeof(insem_cuda_dofmap), sizeof(insem_cuda_domain), sizeof(insem_cuda_coupling),
+         sizeof(insem_cuda_stf), sizeof(insem_cuda_source), sizeof(insem_cuda_receiver), sizeof(insem_cuda_problem),
+         sizeof(insem_cuda_options), offsetof(insem_cuda_problem, dt), sizeof(insem_cuda_time),
+         offsetof(insem_cuda_time, n_steps), offsetof(insem_cuda_time, duration));
   return 0;
 }
 '''
@@ -63,7 +64,8 @@ int main(void) {
         subprocess.run(["gcc", "-I", str(REPO / "include"), cfile, "-o", exe], check=True)
         sizes = [int(x) for x in subprocess.run([exe], capture_output=True, text=True).stdout.split()]
     ours = [C.sizeof(t) for t in (N.Basis, N.Block, N.DofMap, N.Domain, N.Coupling, N.Stf, N.Source,
-                                  N.Receiver, N.Problem, N.Options)] + [N.Problem.dt.offset]
+                                  N.Receiver, N.Problem, N.Options)] + [N.Problem.dt.offset, C.sizeof(N.Time),
+                                                                        N.Time.n_steps.offset, N.Time.duration.offset]
     assert sizes == ours
 
 
@@ -87,3 +89,16 @@ def test_algorithmic_bytes_c1(pkg):
     prob = pkg.ProblemData.from_npz(golden("c1"))
     # 16,641 points x 20 B + 1024 Rect acoustic elements x (4*25 + 12 + 4*25) B
     assert prob.algorithmic_bytes_per_step() == 16641 * 20 + 1024 * (100 + 12 + 100)
+
+
+def test_timed_constructor_rejects_null_arguments(pkg):
+    """Argument checks of insem_cuda_solver_create_timed come before any device work."""
+    from insem_b200 import native as N
+
+    L = pkg.lib()
+    t = N.Time(0.0, 0.8, 0, 1e-3)
+    h = C.c_void_p()
+    assert L.insem_cuda_solver_create_timed(None, C.byref(t), None, C.byref(h)) == N.ERR_INVALID
+    assert b"null" in L.insem_cuda_last_error()
+    assert not h.value
+    assert L.insem_cuda_solver_stable_dt(None) == 0.0
