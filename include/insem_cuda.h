@@ -16,9 +16,9 @@
  *   insem_cuda_solver_*    solver::Solver (cpp/include/insem/solver/solver.hpp:91-228):
  *                          advance / run / set_state / traces / energy / state
  *   insem_cuda_stable_dt   Solver::estimate_stable_dt + coupled_lambda_max
- *   insem_cuda_solver_create_timed  Solver::Solver's stable-dt and dt / n_steps
- *                          rule (solver.cpp:131-144)
  *                          (cpp/src/solver/solver.cpp:583-667), FP64 reductions
+ *   insem_cuda_solver_create_timed  Solver::Solver's stable-dt and dt / n_steps
+ *                          rule (cpp/src/solver/solver.cpp:131-144)
  *   insem_cuda_batch_*     many independent solves advanced by shared launches
  *                          (the serving loop admits and retires solves through it)
  *
@@ -39,6 +39,10 @@
  *
  * Threading: handles are independent; one handle is used by one thread at a
  * time (the reference drives a Solver from one thread, bindings.cpp:336-337).
+ *
+ * Streams: a `stream` argument of NULL means the calling thread's default
+ * stream (the library is built with per-thread default streams), which CUDA
+ * keeps ordered with the legacy default stream in both directions.
  */
 #ifndef INSEM_CUDA_H
 #define INSEM_CUDA_H
