@@ -118,7 +118,7 @@ struct TileHdr {
 struct TiledDev {
   int32_t ng = 0;          // points
   int32_t n_complete = 0;  // complete points are [0, n_complete)
-  int32_t n_hbuf = 0;      // halo buffer entries (per component)
+  int32_t n_hbuf = 0;      // halo contributions (per component): the halo points' lists, point by point
   int32_t n_cslots = 0;    // constrained slots of the domain
   const float* inv_mass = nullptr;
   const float* mass = nullptr;
@@ -131,10 +131,13 @@ struct TiledDev {
   const TileHdr* tiles = nullptr;
   const int32_t* halo_tp = nullptr; // device point of each halo tile point
   const int32_t* hs_slot = nullptr; // tile-local slot (e * npe + k) of each halo entry
+  const int32_t* hs_dst = nullptr;  // its place in hbuf, or -1 - m: the places mdst[mdst_off[m] ..)
+  const int32_t* mdst_off = nullptr;  // entries with several places (constrained slots feeding several points)
+  const int32_t* mdst = nullptr;
   const int32_t* cs_slot = nullptr; // tile-local slot of each constrained slot
   const int32_t* cs_idx = nullptr;  // its index into cval
   const float* cval = nullptr;      // [ncomp][n_cslots] gathered constrained-slot values
-  float* hbuf = nullptr;            // [ncomp][n_hbuf]
+  float* hbuf = nullptr;            // [ncomp][n_hbuf], each halo point's contributions in its slot order
 };
 
 struct StepScalars {
@@ -641,13 +644,25 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     __syncthreads();
   }
 
-  // 6. halo contributions out (hbuf order = ascending slot order within the tile)
+  // 6. halo contributions out, each to its place in its halo point's list
   for (int q = tid; q < th.nhs; q += nthreads) {
     const int32_t ls = td.hs_slot[th.hs_off + q];
+    const int32_t dst = td.hs_dst[th.hs_off + q];
     const int e = ls / NPE, k = ls - e * NPE;
+    float val[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c)
-      td.hbuf[static_cast<size_t>(c) * td.n_hbuf + th.hb + q] = stage[(e * NC + c) * NPE + k];
+    for (int c = 0; c < NC; ++c) val[c] = stage[(e * NC + c) * NPE + k];
+    if (dst >= 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) td.hbuf[static_cast<size_t>(c) * td.n_hbuf + dst] = val[c];
+    } else {
+      const int32_t mi = -1 - dst;
+      for (int32_t d = td.mdst_off[mi]; d < td.mdst_off[mi + 1]; ++d) {
+        const int32_t p = td.mdst[d];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) td.hbuf[static_cast<size_t>(c) * td.n_hbuf + p] = val[c];
+      }
+    }
   }
 
   if (L.late) {
@@ -793,8 +808,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
 // Special-point records of a domain's halo points.
 struct HaloDev {
   int32_t n = 0;                     // halo points: device points [n_complete, n_complete + n)
-  const int32_t* off = nullptr;      // [n+1] halo-buffer contributions, ascending slot order
-  const int32_t* pos = nullptr;      // halo-buffer entry of each contribution
+  const int32_t* off = nullptr;      // [n+1] each point's contributions in hbuf, ascending slot order
   const float* w = nullptr;          // its weight (constrained maps), nullptr when all are 1
   const int32_t* spec = nullptr;     // [n] special record or -1
   const int32_t* src_off = nullptr;  // [n_spec+1] source contributions of each record
@@ -847,14 +861,11 @@ __device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev
     const int32_t b = hd.off[h], e = hd.off[h + 1];
     constexpr int K = 4;  // contributions gathered at once (conforming 2D points have at most 4)
     if (e - b <= K) {
-      int32_t pq[K];
-#pragma unroll
-      for (int q = 0; q < K; ++q) pq[q] = b + q < e ? hd.pos[b + q] : 0;
       float vq[NC][K];
 #pragma unroll
       for (int q = 0; q < K; ++q)
 #pragma unroll
-        for (int c = 0; c < NC; ++c) vq[c][q] = b + q < e ? td.hbuf[static_cast<size_t>(c) * td.n_hbuf + pq[q]] : 0.0f;
+        for (int c = 0; c < NC; ++c) vq[c][q] = b + q < e ? td.hbuf[static_cast<size_t>(c) * td.n_hbuf + b + q] : 0.0f;
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         float s = 0.0f;
@@ -868,7 +879,7 @@ __device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev
       for (int c = 0; c < NC; ++c) {
         float s = 0.0f;
         for (int32_t q = b; q < e; ++q) {
-          const float v = td.hbuf[static_cast<size_t>(c) * td.n_hbuf + hd.pos[q]];
+          const float v = td.hbuf[static_cast<size_t>(c) * td.n_hbuf + q];
           s = fadd(s, hd.w ? fmul(hd.w[q], v) : v);
         }
         f[c] = s;

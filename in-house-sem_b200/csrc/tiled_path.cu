@@ -221,6 +221,9 @@ TiledDev TiledDomain::view(int parity) const {
   t.tiles = tiles.get();
   t.halo_tp = halo_tp.get();
   t.hs_slot = hs_slot.get();
+  t.hs_dst = hs_dst.get();
+  t.mdst_off = mdst_off.get();
+  t.mdst = mdst.get();
   t.cs_slot = cs_slot.get();
   t.cs_idx = cs_idx.get();
   t.cval = cval.get();
@@ -232,7 +235,6 @@ HaloDev TiledDomain::halo_view() const {
   HaloDev h;
   h.n = n_halo;
   h.off = h_off.get();
-  h.pos = h_pos.get();
   h.w = weighted ? h_w.get() : nullptr;
   h.spec = h_spec.get();
   h.src_off = src_off.get();
@@ -452,7 +454,7 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
     }
     e_running += be;
   }
-  n_hbuf = hb;
+  const int32_t n_entries = hb;
   n_cslots = static_cast<int32_t>(crow.size());
   tp_cap = 4;
   nc_cap = 4;
@@ -496,18 +498,44 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
     zm.push_back(iz == sp.zero.end() ? 0 : iz->second);
   }
 
+  // Places of the halo-buffer entries in hbuf: hbuf holds each halo point's
+  // contributions in its ascending slot order, point after point (the list
+  // hoff indexes), so the halo kernel reads them contiguously.  An entry has
+  // one place, unless it is a constrained slot feeding several parent
+  // points; those entries keep a list of places.
+  n_hbuf = static_cast<int32_t>(hpos.size());
+  std::vector<int32_t> ecount(n_entries, 0);
+  for (int32_t e : hpos) ++ecount[e];
+  std::vector<int32_t> hdst(n_entries, 0), moff{0}, mlist;
+  {
+    std::vector<std::vector<int32_t>> multi(n_entries);
+    for (int32_t q = 0; q < n_hbuf; ++q) {
+      const int32_t e = hpos[q];
+      if (ecount[e] == 1) hdst[e] = q;
+      else multi[e].push_back(q);
+    }
+    for (int32_t e = 0; e < n_entries; ++e) {
+      if (ecount[e] == 1) continue;
+      hdst[e] = -1 - (static_cast<int32_t>(moff.size()) - 1);
+      mlist.insert(mlist.end(), multi[e].begin(), multi[e].end());
+      moff.push_back(static_cast<int32_t>(mlist.size()));
+    }
+  }
+
   // 7. uploads
   sdesc.upload(desc);
   tiles.upload(hdr);
   halo_tp.upload(htp.empty() ? std::vector<int32_t>{0} : htp);
   hs_slot.upload(hslot.empty() ? std::vector<int32_t>{0} : hslot);
+  hs_dst.upload(hdst.empty() ? std::vector<int32_t>{0} : hdst);
+  mdst_off.upload(moff);
+  mdst.upload(mlist.empty() ? std::vector<int32_t>{0} : mlist);
   cs_slot.upload(cslot.empty() ? std::vector<int32_t>{0} : cslot);
   cs_idx.upload(cidx.empty() ? std::vector<int32_t>{0} : cidx);
   cs_row.upload(crow.empty() ? std::vector<int32_t>{0} : crow);
   cval.resize(static_cast<std::size_t>(ncomp) * std::max(n_cslots, 1));
   hbuf.resize(static_cast<std::size_t>(ncomp) * std::max(n_hbuf, 1));
   h_off.upload(hoff);
-  h_pos.upload(hpos.empty() ? std::vector<int32_t>{0} : hpos);
   if (weighted) h_w.upload(hw.empty() ? std::vector<float>{0.0f} : hw);
   h_spec.upload(hspec.empty() ? std::vector<int32_t>{0} : hspec);
   src_off.upload(soff);

@@ -42,10 +42,10 @@ class TiledDomain {
   // device data
   DeviceBuffer<uint32_t> sdesc;
   DeviceBuffer<TileHdr> tiles;
-  DeviceBuffer<int32_t> halo_tp, hs_slot, cs_slot, cs_idx, cs_row;
+  DeviceBuffer<int32_t> halo_tp, hs_slot, hs_dst, mdst_off, mdst, cs_slot, cs_idx, cs_row;
   DeviceBuffer<float> cval, hbuf, mass, inv_mass;
   DeviceBuffer<float> u0, u1, v, a, vn;
-  DeviceBuffer<int32_t> h_off, h_pos, h_spec, src_off, src_which, cpl_off, cpl_idx, abs_idx;
+  DeviceBuffer<int32_t> h_off, h_spec, src_off, src_which, cpl_off, cpl_idx, abs_idx;
   DeviceBuffer<float> h_w, src_coef, abs_coef_d;
   DeviceBuffer<uint8_t> zero;
   DeviceBuffer<int32_t> rows_off, rows_dofs;  // constraint rows in device numbering
