@@ -108,6 +108,9 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
   CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CUDA_CHECK(cudaEventCreate(&ev0));
   CUDA_CHECK(cudaEventCreate(&ev1));
+  CUDA_CHECK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  CUDA_CHECK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+  CUDA_CHECK(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
   check_ngll(p.basis.ngll);
   ngll = p.basis.ngll;
   INSEM_REQUIRE(p.n_domains >= 1 && p.n_domains <= 2, INSEM_CUDA_ERR_INVALID, "a problem has 1 or 2 domains");
@@ -185,6 +188,12 @@ Solver::~Solver() {
   device_free(st);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (fork_ev) cudaEventDestroy(fork_ev);
+  if (join_ev) cudaEventDestroy(join_ev);
+  if (side) {
+    cudaStreamSynchronize(side);
+    cudaStreamDestroy(side);
+  }
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -938,6 +947,13 @@ void Solver::enqueue_tiled(int par, bool init) {
       CUDA_LAUNCH_CHECK();
     }
   }
+  // the fluid's tiles beside the solid's: neither reads what the other
+  // writes (the solid's halo kernel reads the fluid's current field only)
+  const bool split = solid >= 0 && fluid >= 0;
+  if (split) {
+    CUDA_CHECK(cudaEventRecord(fork_ev, stream));
+    CUDA_CHECK(cudaStreamWaitEvent(side, fork_ev, 0));
+  }
   for (int di : {solid, fluid}) {
     if (di < 0) continue;
     TiledDomain& t = tdom[di];
@@ -950,9 +966,13 @@ void Solver::enqueue_tiled(int par, bool init) {
       a.st = st;
       a.epartial = epart.get() + 2 * static_cast<std::size_t>(ep_tile[di]);
       a.elastic = t.medium == INSEM_ELASTIC;
-      a.stream = stream;
+      a.stream = split && di == fluid ? side : stream;
       launch_tiles(ngll, a);
     }
+  }
+  if (split) {
+    CUDA_CHECK(cudaEventRecord(join_ev, side));
+    CUDA_CHECK(cudaStreamWaitEvent(stream, join_ev, 0));
   }
   const double h_damp = init ? 0.0 : 0.5 * dt;
   CouplingDev cp{tcpl_fluid.get(), tcpl_solid.get(), cpl_cx.get(), cpl_cz.get()};

@@ -132,6 +132,11 @@ class Solver {
   StepState* st = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // Coupled models: the fluid's tile launches run on `side`, beside the
+  // solid's (neither reads what the other writes), forked after the step's
+  // first kernels and joined before the halo kernels.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
 
   // ------------------------------------------------------ tiled fused path
  public:
