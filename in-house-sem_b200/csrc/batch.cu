@@ -202,6 +202,9 @@ Batch::Batch(const insem_cuda_options* opt) {
   CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CUDA_CHECK(cudaEventCreate(&ev0));
   CUDA_CHECK(cudaEventCreate(&ev1));
+  CUDA_CHECK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  CUDA_CHECK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
+  CUDA_CHECK(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
   CUDA_CHECK(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, opts.device));
   CUDA_CHECK(cudaMallocHost(&herr, sizeof(int32_t)));
   derr.resize(1);
@@ -215,6 +218,12 @@ Batch::~Batch() {
   if (herr) cudaFreeHost(herr);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
+  if (fork_ev) cudaEventDestroy(fork_ev);
+  if (join_ev) cudaEventDestroy(join_ev);
+  if (side) {
+    cudaStreamSynchronize(side);
+    cudaStreamDestroy(side);
+  }
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -379,6 +388,13 @@ void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
     CUDA_LAUNCH_CHECK();
   }
   if (tiles_begin) CUDA_CHECK(cudaEventRecord(tiles_begin, stream));
+  bool any_el = false, any_ac = false;
+  for (const DevClass& d : dclasses) (d.elastic ? any_el : any_ac) = true;
+  const bool split = any_el && any_ac;
+  if (split) {
+    CUDA_CHECK(cudaEventRecord(fork_ev, stream));
+    CUDA_CHECK(cudaStreamWaitEvent(side, fork_ev, 0));
+  }
   for (int32_t q = 0; q < nq; ++q) {
     const DevClass& d = dclasses[q];
     TileBatchLaunch a;
@@ -393,8 +409,12 @@ void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
     a.L = d.L;
     a.smem = d.L.total;
     a.grid = d.grid;
-    a.stream = stream;
+    a.stream = split && !d.elastic ? side : stream;
     tile_batch(d.ngll, a, true);
+  }
+  if (split) {
+    CUDA_CHECK(cudaEventRecord(join_ev, side));
+    CUDA_CHECK(cudaStreamWaitEvent(stream, join_ev, 0));
   }
   if (tiles_end) CUDA_CHECK(cudaEventRecord(tiles_end, stream));
   // solid halos first: the fluid's coupling term reads the solid's new acceleration

@@ -116,6 +116,11 @@ class Batch {
 
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // acoustic tile classes run on `side`, beside the elastic ones (neither
+  // reads what the other writes), forked after the constrained gathers and
+  // joined before the halo kernels
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
   int n_sms = 0;
   std::vector<std::unique_ptr<insem_cuda_solver>> members;  // null after remove()
   std::vector<char> prepared;
