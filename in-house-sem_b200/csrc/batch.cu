@@ -212,7 +212,9 @@ Batch::Batch(const insem_cuda_options* opt) {
 
 Batch::~Batch() {
   DeviceGuard dg(opts.device);
+  // members' buffers are released below: both streams must be done with them
   if (stream) cudaStreamSynchronize(stream);
+  if (side) cudaStreamSynchronize(side);
   if (graph) cudaGraphExecDestroy(graph);
   members.clear();
   if (herr) cudaFreeHost(herr);
@@ -220,10 +222,7 @@ Batch::~Batch() {
   if (ev1) cudaEventDestroy(ev1);
   if (fork_ev) cudaEventDestroy(fork_ev);
   if (join_ev) cudaEventDestroy(join_ev);
-  if (side) {
-    cudaStreamSynchronize(side);
-    cudaStreamDestroy(side);
-  }
+  if (side) cudaStreamDestroy(side);
   if (stream) cudaStreamDestroy(stream);
 }
 

@@ -181,7 +181,9 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
 
 Solver::~Solver() {
   DeviceGuard dg(device);
-  if (stream) cudaStreamSynchronize(stream);  // buffers go back to the pool below
+  // buffers go back to the pool below: both streams must be done with them
+  if (stream) cudaStreamSynchronize(stream);
+  if (side) cudaStreamSynchronize(side);
   if (graph_exec) cudaGraphExecDestroy(graph_exec);
   for (auto& g : tgraph)
     if (g) cudaGraphExecDestroy(g);
@@ -190,10 +192,7 @@ Solver::~Solver() {
   if (ev1) cudaEventDestroy(ev1);
   if (fork_ev) cudaEventDestroy(fork_ev);
   if (join_ev) cudaEventDestroy(join_ev);
-  if (side) {
-    cudaStreamSynchronize(side);
-    cudaStreamDestroy(side);
-  }
+  if (side) cudaStreamDestroy(side);
   if (stream) cudaStreamDestroy(stream);
 }
 
