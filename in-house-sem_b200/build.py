@@ -69,14 +69,18 @@ def compile_unit(src: Path, extra: list[str], obj: Path, verbose: bool, force: b
 
 
 def build_cases(force: bool = False) -> Path:
-    """Host-only case-setup library (csrc/host), compiled with the system C++ compiler."""
-    src = CSRC / "host" / "cases.cpp"
-    hdr = CSRC / "host" / "insem_cases.h"
-    if force or not CASES_LIB.exists() or CASES_LIB.stat().st_mtime < max(src.stat().st_mtime, hdr.stat().st_mtime):
+    """Host-only case-setup library (csrc/host), compiled with the system C++
+    compiler.  No contraction to fused multiply-adds, so every double the
+    setup forms rounds like the reference's setup code."""
+    host = CSRC / "host"
+    srcs = sorted(host.glob("*.cpp"))
+    newest = max(p.stat().st_mtime for p in srcs + sorted(host.glob("*.h")) + sorted(host.glob("*.hpp")))
+    if force or not CASES_LIB.exists() or CASES_LIB.stat().st_mtime < newest:
         CASES_LIB.parent.mkdir(parents=True, exist_ok=True)
         cxx = shutil.which("g++") or "c++"
         tmp = CASES_LIB.with_suffix(".so.tmp")
-        cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", str(src), "-o", str(tmp)]
+        cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", "-ffp-contract=off",
+               *[str(s) for s in srcs], "-o", str(tmp)]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"case library build failed:\n{res.stderr[-6000:]}")

@@ -6,9 +6,9 @@ cpp/include/insem/sim/simulation.hpp:56-124); ``build`` runs the native
 setup (csrc/host/cases.cpp) and the device power iteration for the stable
 time step, and returns the ``ProblemData`` the solver takes.
 
-The mesh templates follow the node-lattice, cell-ordering and boundary-tag
-conventions of the reference's python/insem/mesh/templates.py (BOTTOM 1,
-RIGHT 2, TOP 3, LEFT 4; Quad9 cells honour curved interfaces).
+The mesh templates (rectangle, layered, borehole) produce the macro meshes
+of the reference's templates (python/insem/mesh/templates.py) node for node,
+so that a model described here and through the reference set up identically.
 
 Workloads (seeded; shapes and value ranges as the benchmark configurations
 state them):
@@ -34,10 +34,19 @@ BOTTOM, RIGHT, TOP, LEFT = 1, 2, 3, 4
 MEDIUM = {"acoustic": 0, "elastic": 1}
 BC = {"free": 0, "rigid": 1, "absorbing": 2}
 SOURCE_KIND = {"force": 0, "moment_tensor": 1, "monopole": 2, "dipole": 3}
-STF_KIND = {"ricker": 0, "gaussian": 1, "gaussian_derivative": 2}
+STF_KIND = {"ricker": 0, "gaussian": 1, "gaussian_derivative": 2, "samples": 3}
 
 
 # ------------------------------------------------------------------ meshes
+# Structured macro meshes.  Cells are numbered row by row (x fastest), corners
+# counter-clockwise from (-1, -1), Quad9 side midpoints then the centre; the
+# boundary sides carry the tags BOTTOM 1, RIGHT 2, TOP 3, LEFT 4, listed per
+# cell in side order.  These are the conventions of the reference's mesh
+# templates (python/insem/mesh/templates.py), whose node coordinates the
+# builder tests require bit for bit: breakpoints are np.linspace, Quad9
+# midpoints the mean of their two breakpoints, layer rows the linear blend
+# (1 - t) z_bottom + t z_top with t = row / rows, radial grading the running
+# sum of geometrically growing sizes.
 @dataclass
 class MacroMesh:
     quad9: bool
@@ -48,99 +57,99 @@ class MacroMesh:
     boundary: np.ndarray   # (n_faces, 3) cell, face, tag
 
 
-def _lattice(breaks: np.ndarray, quadratic: bool) -> np.ndarray:
-    if not quadratic:
-        return breaks
-    out = np.empty(2 * breaks.size - 1)
-    out[0::2] = breaks
-    out[1::2] = 0.5 * (breaks[:-1] + breaks[1:])
-    return out
-
-
-def _structured(xl: np.ndarray, zl: np.ndarray, quadratic: bool, region: np.ndarray, axisym: bool) -> MacroMesh:
-    """Cells row by row (x fastest) over a node lattice: xl (mx,), zl (mz, mx)."""
-    step = 2 if quadratic else 1
-    mx = xl.size
-    ncx, ncz = (mx - 1) // step, (zl.shape[0] - 1) // step
-    if np.any(np.diff(zl, axis=0) <= 0):
-        raise ValueError("layer interfaces must increase in z at every x")
-    nodes = np.column_stack([np.broadcast_to(xl, zl.shape).ravel(), zl.ravel()])
-    jj, ii = np.meshgrid(np.arange(ncz), np.arange(ncx), indexing="ij")
-    a, b = (step * ii).ravel(), (step * jj).ravel()
-
-    def node(i, j):
-        return i + mx * j
-
-    if quadratic:
-        cells = np.stack([node(a, b), node(a + 2, b), node(a + 2, b + 2), node(a, b + 2), node(a + 1, b),
-                          node(a + 2, b + 1), node(a + 1, b + 2), node(a, b + 1), node(a + 1, b + 1)], axis=1)
-    else:
-        cells = np.stack([node(a, b), node(a + 1, b), node(a + 1, b + 1), node(a, b + 1)], axis=1)
-    c = np.arange(ncx * ncz)
-    i, j = c % ncx, c // ncx
-    faces = []
-    for cond, face, tag in ((j == 0, 0, BOTTOM), (i == ncx - 1, 1, RIGHT), (j == ncz - 1, 2, TOP), (i == 0, 3, LEFT)):
-        sel = c[cond]
-        faces.append(np.stack([sel, np.full(sel.size, face), np.full(sel.size, tag), sel * 4 + face], axis=1))
-    f = np.concatenate(faces)
-    f = f[np.argsort(f[:, 3], kind="stable")][:, :3]  # per cell in face order, as the template loops
-    return MacroMesh(quadratic, axisym, np.ascontiguousarray(nodes, float), np.ascontiguousarray(cells, np.int32),
-                     np.ascontiguousarray(region, np.int32), np.ascontiguousarray(f, np.int32))
-
-
-def _axis(spec, n: Optional[int]) -> np.ndarray:
+def _breakpoints(spec, cells: Optional[int]) -> np.ndarray:
+    """Either explicit breakpoints, or (lo, hi) split into `cells` equal cells."""
     v = np.asarray(spec, float)
-    return v if n is None else np.linspace(v[0], v[1], n + 1)
+    return v if cells is None else np.linspace(v[0], v[1], cells + 1)
+
+
+def _node_positions(breaks: np.ndarray, quad9: bool) -> np.ndarray:
+    """Node positions along one direction: the breakpoints, and for Quad9 cells
+    the midpoint of every interval between them."""
+    if not quad9:
+        return breaks
+    mids = (breaks[:-1] + breaks[1:]) * 0.5
+    return np.append(np.column_stack([breaks[:-1], mids]).ravel(), breaks[-1])
+
+
+_QUAD9_OFFSETS = np.array([(0, 0), (2, 0), (2, 2), (0, 2), (1, 0), (2, 1), (1, 2), (0, 1), (1, 1)])
+_QUAD4_OFFSETS = np.array([(0, 0), (1, 0), (1, 1), (0, 1)])
+
+
+def _grid_mesh(columns: np.ndarray, heights: np.ndarray, quad9: bool, region: np.ndarray, axisym: bool) -> MacroMesh:
+    """Macro mesh on a node grid: `columns` (m,) x positions, `heights` (rows, m)
+    node z per grid row."""
+    stride = 2 if quad9 else 1
+    m = columns.size
+    ncx, ncz = (m - 1) // stride, (heights.shape[0] - 1) // stride
+    if np.any(np.diff(heights, axis=0) <= 0):
+        raise ValueError("grid rows must rise strictly in z at every x (zero-thickness layers?)")
+    nodes = np.column_stack([np.tile(columns, heights.shape[0]), heights.ravel()])
+    c = np.arange(ncx * ncz)
+    ci, cj = c % ncx, c // ncx
+    off = _QUAD9_OFFSETS if quad9 else _QUAD4_OFFSETS
+    cells = (stride * ci[:, None] + off[None, :, 0]) + m * (stride * cj[:, None] + off[None, :, 1])
+    # boundary sides: (cell, side, tag), ordered by cell then side
+    sides = np.stack([cj == 0, ci == ncx - 1, cj == ncz - 1, ci == 0], axis=1)
+    cell_of, side_of = np.nonzero(sides)
+    tags = np.array([BOTTOM, RIGHT, TOP, LEFT])[side_of]
+    boundary = np.column_stack([cell_of, side_of, tags])
+    return MacroMesh(quad9, axisym, np.ascontiguousarray(nodes, float), np.ascontiguousarray(cells, np.int32),
+                     np.ascontiguousarray(region, np.int32), np.ascontiguousarray(boundary, np.int32))
 
 
 def rectangle(x, z, nx=None, nz=None, material: Union[int, Sequence[int], Callable] = 0, quadratic=False,
               coords="cartesian") -> MacroMesh:
-    xs, zs = _axis(x, nx), _axis(z, nz)
-    ncx, ncz = xs.size - 1, zs.size - 1
-    xl = _lattice(xs, quadratic)
-    zl = np.repeat(_lattice(zs, quadratic)[:, None], xl.size, axis=1)
+    """Rectangle of nx x nz cells (or explicit breakpoints); `material` is a
+    region id, one id per cell, or f(x_centre, z_centre) -> id (vectorised when
+    the function has ``vectorized = True``)."""
+    xb, zb = _breakpoints(x, nx), _breakpoints(z, nz)
+    ncx, ncz = xb.size - 1, zb.size - 1
+    cols = _node_positions(xb, quadratic)
+    rows = np.repeat(_node_positions(zb, quadratic)[:, None], cols.size, axis=1)
     if callable(material):
-        xc, zc = 0.5 * (xs[:-1] + xs[1:]), 0.5 * (zs[:-1] + zs[1:])
-        if getattr(material, "vectorized", False):  # takes the cell-centre arrays (row-major, x fastest)
-            X, Z = np.meshgrid(xc, zc)
-            mat = np.asarray(material(X.ravel(), Z.ravel()), np.int32)
+        xc = np.tile((xb[:-1] + xb[1:]) * 0.5, ncz)
+        zc = np.repeat((zb[:-1] + zb[1:]) * 0.5, ncx)
+        if getattr(material, "vectorized", False):
+            region = np.asarray(material(xc, zc), np.int32)
         else:
-            mat = np.array([material(xc[i], zc[j]) for j in range(ncz) for i in range(ncx)], np.int32)
+            region = np.array([material(a, b) for a, b in zip(xc, zc)], np.int32)
     else:
-        mat = np.broadcast_to(np.asarray(material, np.int32), (ncx * ncz,)).copy()
-    return _structured(xl, zl, quadratic, mat, coords == "axisymmetric")
+        region = np.broadcast_to(np.asarray(material, np.int32), (ncx * ncz,)).copy()
+    return _grid_mesh(cols, rows, quadratic, region, coords == "axisymmetric")
 
 
 def layered(x, interfaces, nz, regions, nx=None, quadratic=False, coords="cartesian") -> MacroMesh:
-    """Layers between K + 1 interfaces (constants or callables z(x)), bottom to top."""
-    xs = _axis(x, nx)
-    k = len(interfaces) - 1
-    counts = [int(nz)] * k if np.isscalar(nz) else [int(v) for v in nz]
-    xl = _lattice(xs, quadratic)
-    levels = [np.broadcast_to(np.asarray(i(xl) if callable(i) else float(i), float), xl.shape).astype(float)
-              for i in interfaces]
-    step = 2 if quadratic else 1
-    rows = [levels[0]]
-    for layer in range(k):
-        n_rows = step * counts[layer]
-        for r in range(1, n_rows + 1):
-            t = r / n_rows
-            rows.append((1.0 - t) * levels[layer] + t * levels[layer + 1])
-    zl = np.vstack(rows)
-    ncx = xs.size - 1
-    mat = np.concatenate([np.full(ncx * counts[layer], regions[layer], np.int32) for layer in range(k)])
-    return _structured(xl, zl, quadratic, mat, coords == "axisymmetric")
+    """Layers between K + 1 interfaces (heights or vectorised z(x)), bottom to
+    top, with nz cells across each (one count or K counts) and region ids
+    `regions`; node rows inside a layer blend its two interfaces linearly."""
+    xb = _breakpoints(x, nx)
+    cols = _node_positions(xb, quadratic)
+    n_layers = len(interfaces) - 1
+    counts = [int(nz)] * n_layers if np.isscalar(nz) else [int(v) for v in nz]
+    surfaces = [np.broadcast_to(np.asarray(f(cols) if callable(f) else float(f), float), cols.shape).astype(float)
+                for f in interfaces]
+    stride = 2 if quadratic else 1
+    blocks = [surfaces[0][None, :]]
+    for k in range(n_layers):
+        steps = stride * counts[k]
+        t = (np.arange(1, steps + 1) / steps)[:, None]
+        blocks.append((1.0 - t) * surfaces[k][None, :] + t * surfaces[k + 1][None, :])
+    region = np.repeat(np.asarray(regions[:n_layers], np.int32), [(xb.size - 1) * c for c in counts])
+    return _grid_mesh(cols, np.vstack(blocks), quadratic, region, coords == "axisymmetric")
 
 
-def _graded(r0, r1, first, growth, max_size) -> List[float]:
-    out, r, size = [r0], r0, first
-    while r1 - r > 1e-12 * max(1.0, abs(r1)):
-        size = min(size, max_size)
-        if r1 - r <= 1.5 * size:
-            out.append(r1)
+def _grown_breaks(start: float, stop: float, first: float, growth: float, cap: float) -> List[float]:
+    """Breakpoints from start to stop for cells of size first, first * growth,
+    ... (at most cap); a remainder shorter than 1.5 cells joins the last one."""
+    out = [start]
+    size = first
+    while stop - out[-1] > 1e-12 * max(1.0, abs(stop)):
+        size = min(size, cap)
+        if stop - out[-1] <= 1.5 * size:
+            out.append(stop)
             break
-        r += size
-        out.append(r)
+        out.append(out[-1] + size)
         size *= growth
     return out
 
@@ -154,41 +163,49 @@ class Borehole:
 
 def borehole(z, annuli, formation_radius, beds=(), dz=0.05, dr=None, growth=1.3, fluid_cells=2,
              quadratic=False) -> Borehole:
-    """Axisymmetric borehole: annuli around the axis, graded formation split into beds."""
+    """Axisymmetric (r, z) borehole: `annuli` = [(name, outer radius), ...] from
+    the axis out (the fluid column gets `fluid_cells` radial cells, the others
+    about one cell per dz), then the formation out to `formation_radius` with
+    cells growing by `growth` up to `dr` (default 4 dz), split into `beds` =
+    [(z_bottom, name), ...].  Region ids count from 1 in order of first
+    appearance, annuli before beds; tags: bottom 1, outer 2, top 3, axis 4."""
     z0, z1 = float(z[0]), float(z[1])
-    radii = [float(r) for _, r in annuli]
+    names = [a for a, _ in annuli]
+    outer = [float(r) for _, r in annuli]
     beds = list(beds) or [(z0, "formation")]
-    dr = 4 * dz if dr is None else dr
-    r_breaks = list(np.linspace(0.0, radii[0], fluid_cells + 1))
-    last = radii[0] / fluid_cells
-    for inner, outer in zip(radii, radii[1:]):
-        n = max(1, int(np.ceil((outer - inner) / dz - 1e-9)))
-        r_breaks += list(np.linspace(inner, outer, n + 1)[1:])
-        last = (outer - inner) / n
-    r_breaks += _graded(radii[-1], formation_radius, min(last * growth, dr), growth, dr)[1:]
-    tops = [b[0] for b in beds[1:]] + [z1]
-    z_breaks = [z0]
-    for bottom, top in zip([b[0] for b in beds], tops):
-        n = max(1, int(np.ceil((top - bottom) / dz - 1e-9)))
-        z_breaks += list(np.linspace(bottom, top, n + 1)[1:])
-    names: Dict[str, int] = {}
-    for name in [a for a, _ in annuli] + [b for _, b in beds]:
-        names.setdefault(name, len(names) + 1)
-    bottoms = np.array([b[0] for b in beds])
+    cap = 4 * dz if dr is None else dr
 
-    bed_ids = np.array([names[b[1]] for b in beds], np.int32)
+    def cells_across(a: float, b: float) -> int:
+        return max(1, int(np.ceil((b - a) / dz - 1e-9)))
+
+    r = list(np.linspace(0.0, outer[0], fluid_cells + 1))
+    last_cell = outer[0] / fluid_cells
+    for a, b in zip(outer[:-1], outer[1:]):
+        k = cells_across(a, b)
+        r.extend(np.linspace(a, b, k + 1)[1:])
+        last_cell = (b - a) / k
+    r.extend(_grown_breaks(outer[-1], formation_radius, min(last_cell * growth, cap), growth, cap)[1:])
+
+    bottoms = [float(b[0]) for b in beds]
+    zs = [z0]
+    for a, b in zip(bottoms, bottoms[1:] + [z1]):
+        zs.extend(np.linspace(a, b, cells_across(a, b) + 1)[1:])
+
+    ids = {name: i + 1 for i, name in enumerate(dict.fromkeys(names + [b[1] for b in beds]))}
+    annulus_ids = np.array([ids[n] for n in names], np.int32)
+    bed_ids = np.array([ids[b[1]] for b in beds], np.int32)
+    outer_arr = np.array(outer)
 
     def region(rc, zc):
         rc, zc = np.asarray(rc, float), np.asarray(zc, float)
-        out = bed_ids[np.searchsorted(bottoms, zc, side="right") - 1]
-        for name, outer in reversed(annuli):  # the innermost annulus containing the cell wins
-            out = np.where(rc < outer, names[name], out)
-        return out
+        inside = rc[:, None] < outer_arr[None, :]             # the first annulus whose outer radius exceeds rc
+        ring = np.argmax(inside, axis=1)
+        bed = bed_ids[np.searchsorted(np.array(bottoms), zc, side="right") - 1]
+        return np.where(inside.any(axis=1), annulus_ids[ring], bed)
 
     region.vectorized = True
-
-    m = rectangle(r_breaks, z_breaks, material=region, quadratic=quadratic, coords="axisymmetric")
-    return Borehole(m, names, {"bottom": BOTTOM, "outer": RIGHT, "top": TOP, "axis": LEFT})
+    m = rectangle(r, zs, material=region, quadratic=quadratic, coords="axisymmetric")
+    return Borehole(m, ids, {"bottom": BOTTOM, "outer": RIGHT, "top": TOP, "axis": LEFT})
 
 
 # ------------------------------------------------------------------ model
@@ -219,6 +236,22 @@ class Source:
 
 def ricker(f0, t0=-1.0, amplitude=1.0):
     return ("ricker", f0, t0, amplitude)
+
+
+def gaussian(f0, t0=-1.0, amplitude=1.0):
+    return ("gaussian", f0, t0, amplitude)
+
+
+def gaussian_derivative(f0, t0=-1.0, amplitude=1.0):
+    return ("gaussian_derivative", f0, t0, amplitude)
+
+
+def sampled(samples, dt, amplitude=1.0):
+    """Samples at t = i * dt, linearly interpolated, zero outside [0, (n - 1) dt]."""
+    samples = np.asarray(samples, np.float64)
+    if dt <= 0.0 or samples.size == 0:
+        raise ValueError("a sampled source time function needs samples and a positive interval")
+    return ("samples", 0.0, 0.0, amplitude, samples, float(dt))
 
 
 @dataclass
@@ -320,8 +353,9 @@ def setup_arrays(model: Model) -> Dict[str, np.ndarray]:
         res[f"problem.receivers.{ri}.name"] = np.asarray(r.name)
         res[f"problem.receivers.{ri}.quantities"] = np.asarray(r.quantities, dtype="U32")
     for si in range(len(model.sources)):
-        res[f"problem.sources.{si}.stf.samples"] = np.zeros(0)
-        res[f"problem.sources.{si}.stf.sample_dt"] = np.asarray(0.0)
+        stf = model.sources[si].stf
+        res[f"problem.sources.{si}.stf.samples"] = stf[4] if stf[0] == "samples" else np.zeros(0)
+        res[f"problem.sources.{si}.stf.sample_dt"] = np.asarray(stf[5] if stf[0] == "samples" else 0.0)
     return res
 
 
@@ -359,7 +393,8 @@ def describe(model: Model):
     d.source_position = arr([[s.x, s.z] for s in src], np.float64)
     d.source_components = arr([list(s.components) for s in src], np.float64)
     d.stf_kind = arr([STF_KIND[s.stf[0]] for s in src], np.int32)
-    d.stf_params = arr([[s.stf[1], s.stf[2] if s.stf[2] >= 0 else 1.2 / s.stf[1], s.stf[3]] for s in src], np.float64)
+    d.stf_params = arr([[s.stf[1], s.stf[2] if s.stf[2] >= 0 or s.stf[0] == "samples" else 1.2 / s.stf[1], s.stf[3]]
+                        for s in src], np.float64)
     rec = model.receivers
     d.n_receivers = len(rec)
     d.receiver_position = arr([[r.x, r.z] for r in rec], np.float64)
@@ -445,12 +480,10 @@ def config2(z=(-1.5, 4.5), formation_radius=4.0) -> Model:
                  sources=[Source("monopole", 0.0, 0.0, stf=ricker(8000.0))], receivers=recs, duration=5e-3)
 
 
-def config3(nx: int = 1024, n_steps: int = 2000, seed: int = 3, n_receivers: int = 512) -> Model:
-    """Water (60 m, 154/1024 of the rows) over 8 elastic layers with sinusoidal
-    interfaces (amplitude U(2, 6) m, wavelength U(80, 200) m), 400 m wide, order 5,
-    Quad9 cells; force source at (200, -20) Ricker 30 Hz; velocity receivers on
-    the seafloor; Stacey on sides and bottom, free surface on top.  nx = 1024 is
-    the benchmark size; rows scale with nx."""
+def config3_spec(nx: int = 1024, seed: int = 3, n_receivers: int = 512) -> dict:
+    """The seeded layer stack of the large coupled model as plain data:
+    interfaces (bottom to top; constants or vectorised z(x)), rows per layer,
+    region ids, (vp, vs, rho) per elastic region and the receiver x positions."""
     rng = np.random.default_rng(seed)
     amp = rng.uniform(2.0, 6.0, 7)
     lam = rng.uniform(80.0, 200.0, 7)
@@ -465,13 +498,23 @@ def config3(nx: int = 1024, n_steps: int = 2000, seed: int = 3, n_receivers: int
     rows_water = round(154 * nx / 1024)
     rows_el = nx - rows_water
     counts = [rows_el // 8 + (1 if k < rows_el % 8 else 0) for k in range(8)] + [rows_water]
-    regions = list(range(1, 9)) + [0]
-    m = layered((0.0, 400.0), interfaces, counts, regions, nx=nx, quadratic=True)
+    return dict(interfaces=interfaces, counts=counts, regions=list(range(1, 9)) + [0],
+                elastic={k + 1: (float(vp[k]), float(vs[k]), float(rho[k])) for k in range(8)},
+                receivers_x=[float(x) for x in np.linspace(1.0, 399.0, n_receivers)])
+
+
+def config3(nx: int = 1024, n_steps: int = 2000, seed: int = 3, n_receivers: int = 512) -> Model:
+    """Water (60 m, 154/1024 of the rows) over 8 elastic layers with sinusoidal
+    interfaces (amplitude U(2, 6) m, wavelength U(80, 200) m), 400 m wide, order 5,
+    Quad9 cells; force source at (200, -20) Ricker 30 Hz; velocity receivers on
+    the seafloor; Stacey on sides and bottom, free surface on top.  nx = 1024 is
+    the benchmark size; rows scale with nx."""
+    spec = config3_spec(nx, seed, n_receivers)
+    m = layered((0.0, 400.0), spec["interfaces"], spec["counts"], spec["regions"], nx=nx, quadratic=True)
     mats = {0: Material.acoustic(1500.0, 1000.0)}
-    for k in range(8):
-        mats[k + 1] = Material.elastic(float(vp[k]), float(vs[k]), float(rho[k]))
-    recs = [Receiver(f"sf{i}", float(x), -0.5, ["velocity"], "elastic")
-            for i, x in enumerate(np.linspace(1.0, 399.0, n_receivers))]
+    for region, (vp, vs, rho) in spec["elastic"].items():
+        mats[region] = Material.elastic(vp, vs, rho)
+    recs = [Receiver(f"sf{i}", x, -0.5, ["velocity"], "elastic") for i, x in enumerate(spec["receivers_x"])]
     return Model(m, order=5, materials=mats,
                  boundaries={BOTTOM: "absorbing", LEFT: "absorbing", RIGHT: "absorbing", TOP: "free"},
                  sources=[Source("force", 200.0, -20.0, (0.0, 1.0, 0.0), ricker(30.0))], receivers=recs,
