@@ -16,15 +16,26 @@ check that it agrees bit for bit with the float build on this machine.
 
 Random inputs are regenerated in the tests from the same seeds
 (``numpy.random.default_rng(seed)``), so only outputs are stored.
+
+``--timed`` makes the fixtures of the benchmarked configurations instead
+(``timed_cases.py``: config 2 at its stated geometry, config 3 at 64 x 64,
+six config 4 boreholes, the Gaussian and sampled source time functions).
+Their setup arrays are large, so ``timed_<case>.npz`` stores a SHA-256 digest
+of every problem array and of the final fields, next to the reference's dt,
+stable dt, step counts, receiver traces and energy samples.  The double build
+runs the same model with the float build's dt (so samples align) and writes
+``timed_<case>_f64.npz`` with traces and energy.
 """
 
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import subprocess
 import sys
+import time
 from pathlib import Path
 
 import numpy as np
@@ -147,13 +158,104 @@ def run_variant(variant: str, outdir: Path, only: list[str] | None) -> dict:
     return summary
 
 
+def digest(a) -> str:
+    a = np.ascontiguousarray(np.asarray(a))
+    return hashlib.sha256(a.tobytes()).hexdigest()
+
+
+TRACE_SAMPLES_KEPT = 600
+
+
+def thin_traces(out: dict) -> dict:
+    """Long runs: every trace keeps a SHA-256 digest of all its samples (the
+    bitwise check) and every k-th sample row (the tolerance checks), k chosen
+    so that about TRACE_SAMPLES_KEPT rows remain; the sample times likewise."""
+    n = len(out["run.times"])
+    stride = max(1, -(-n // TRACE_SAMPLES_KEPT))
+    res = dict(out)
+    res["meta.trace_stride"] = np.int64(stride)
+    for k, v in out.items():
+        if k.startswith("run.trace.") or k == "run.times":
+            a = np.ascontiguousarray(np.asarray(v))
+            res[f"hash.{k}"] = np.asarray(digest(a))
+            res[f"shape.{k}"] = np.asarray(a.shape, np.int64)
+            res[k] = a[::stride]
+    return res
+
+
+def run_timed_variant(variant: str, outdir: Path, only: list[str] | None) -> None:
+    sys.path.insert(0, str(REF_BUILD / variant))
+    sys.path.insert(0, str(HERE))
+    sys.path.insert(0, str(REPO))
+    import insem  # noqa: F401  (the reference package, oracle build)
+    import _refdump as rd
+    import timed_cases
+
+    for name, make in timed_cases.TIMED_CASES.items():
+        if only and name not in only:
+            continue
+        t_start = time.time()
+        sim, n_run, model = make()
+        if variant == "double":
+            ref = np.load(outdir / f"timed_{name}.npz")
+            sim.set_time(n_steps=model.n_steps, duration=model.duration, dt=float(ref["meta.dt"]),
+                         safety=model.safety, record_every=model.record_every, energy_every=model.energy_every)
+        solver = sim.solver
+        n_full = int(solver.n_steps)
+        n_run = n_full if n_run <= 0 else min(n_run, n_full)
+        out: dict = {"meta.n_steps_full": np.int64(n_full), "meta.n_steps_run": np.int64(n_run),
+                     "meta.dt": np.float64(solver.dt), "meta.stable_dt": np.float64(solver.stable_dt)}
+        if variant == "float":
+            prob: dict = {}
+            flatten("problem", rd.problem(solver), prob)
+            for k, v in prob.items():
+                a = np.asarray(v)
+                if a.dtype.kind in "US":
+                    out[f"text.{k}"] = a
+                    continue
+                out[f"hash.{k}"] = np.asarray(digest(a))
+                out[f"dtype.{k}"] = np.asarray(a.dtype.str)
+                out[f"size.{k}"] = np.int64(a.size)
+        first = n_run // 3
+        solver.advance(first)
+        solver.advance(n_run - first)
+        out["run.times"] = np.asarray(solver.times)
+        for rec in model.receivers:
+            for q in rec.quantities:
+                out[f"run.trace.{rec.name}.{q}"] = np.asarray(solver.trace(rec.name, q))
+        out["run.energy"] = np.asarray(solver.energy).reshape(-1, 3)
+        if variant == "float":
+            for di in range(len(rd.problem(solver)["domains"])):
+                f = rd.fields(solver, di)
+                for k in ("u", "v", "a"):
+                    a = np.asarray(f[k])
+                    out[f"hash.run.d{di}.{k}"] = np.asarray(digest(a))
+                    out[f"norm.run.d{di}.{k}"] = np.float64(np.linalg.norm(a.astype(np.float64)))
+        suffix = "" if variant == "float" else "_f64"
+        np.savez_compressed(outdir / f"timed_{name}{suffix}.npz", **thin_traces(out))
+        print(f"[{variant}] timed {name}: {n_run} of {n_full} steps, dt {solver.dt:.6e}, "
+              f"{time.time() - t_start:.1f} s", flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--variant", choices=["float", "double", "strict"])
     ap.add_argument("--out", default=str(HERE))
     ap.add_argument("--only", nargs="*")
+    ap.add_argument("--timed", action="store_true", help="fixtures of the benchmarked configurations")
     args = ap.parse_args()
     outdir = Path(args.out)
+    if args.timed:
+        if args.variant:
+            run_timed_variant(args.variant, outdir, args.only)
+            return
+        env = dict(os.environ, PYTHONDONTWRITEBYTECODE="1", OMP_NUM_THREADS=os.environ.get("OMP_NUM_THREADS", "8"))
+        for variant in ("float", "double"):
+            cmd = [sys.executable, __file__, "--timed", "--variant", variant, "--out", str(outdir)]
+            if args.only:
+                cmd += ["--only", *args.only]
+            subprocess.run(cmd, check=True, env=env)
+        return
     if args.variant:
         summary = run_variant(args.variant, outdir, args.only)
         if summary:

@@ -1,0 +1,67 @@
+"""The native case builder against the reference's setup on the benchmarked models (CPU only).
+
+``tests/golden/timed_<case>.npz`` holds a SHA-256 digest of every array the
+reference solver packed for the models of ``tests/golden/timed_models.py``:
+config 2 at its stated geometry, config 3 at 64 x 64 elements, six of the 256
+config 4 boreholes that ``bench.py`` times, and the Gaussian / sampled source
+time function cases.  Every array the native builder produces must hash to the
+same digest once cast to the reference's dtype (integers exactly, floats bit
+for bit).
+"""
+
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+TIMED = ["c2", "c3s", "stfg", "stfs", "c4m0", "c4m1", "c4m12", "c4m17", "c4m72", "c4m80"]
+SKIP = ("problem.dt", "problem.stable_dt", "problem.n_steps", "problem.real_bytes")
+
+
+def timed_fixture(case):
+    return np.load(GOLDEN / f"timed_{case}.npz")
+
+
+def timed_model(case):
+    import sys
+
+    sys.path.insert(0, str(GOLDEN))
+    import timed_models
+
+    return timed_models.TIMED[case]()
+
+
+def digest(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("case", TIMED)
+def test_builder_matches_reference_on_benchmarked_models(pkg, case):
+    from insem_b200 import cases as K
+
+    z = timed_fixture(case)
+    model, _, _ = timed_model(case)
+    arrays = K.setup_arrays(model)
+    checked, mismatched = 0, []
+    for hk in z.files:
+        if not hk.startswith("hash.problem."):
+            continue
+        key = hk[len("hash."):]
+        if key in SKIP or key.endswith(".coords") or key.endswith("trace_index"):
+            continue
+        size = int(z[f"size.{key}"])
+        if key not in arrays:
+            assert size == 0, f"{key}: the builder has no array, the reference has {size} entries"
+            continue
+        v = np.asarray(arrays[key])
+        assert v.size == size, (key, v.size, size)
+        v = v.astype(np.dtype(str(z[f"dtype.{key}"])))
+        if digest(v) != str(z[hk]):
+            mismatched.append(key)
+        checked += 1
+    assert not mismatched, f"arrays differing from the reference's setup: {mismatched[:8]}"
+    assert checked > 20
