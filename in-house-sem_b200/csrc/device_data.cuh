@@ -183,5 +183,7 @@ struct DeviceDofMap {
 // Element-local gather and CSR assemble (DofMap seam), in dofmap_kernels.cu.
 void launch_gather(const DeviceDofMap& d, int ncomp, const float* global, float* local, cudaStream_t s);
 void launch_assemble(const DeviceDofMap& d, int ncomp, const float* local, float* global, cudaStream_t s);
+// Loads assemble_kernel<weighted> (its module, under lazy loading) without launching it.
+void preload_assemble(bool weighted);
 
 }  // namespace insem_b200

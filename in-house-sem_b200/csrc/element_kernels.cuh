@@ -87,6 +87,9 @@ struct ElementLaunch {
   float* f_local = nullptr;
   bool gather = false;
   bool elastic = false;
+  // load the kernel this launch would run (its module, under lazy loading)
+  // without launching it
+  bool preload = false;
   cudaStream_t stream = nullptr;
 };
 
@@ -94,6 +97,12 @@ template <int NG, int KIND, bool ELASTIC, int M>
 void launch_element_cfg(const ElementLaunch& a) {
   using C = ElemCfg<NG, KIND, ELASTIC, M>;
   if (a.blk.n <= 0) return;
+  if (a.preload) {
+    cudaFuncAttributes fa;
+    if (a.gather) CUDA_CHECK(cudaFuncGetAttributes(&fa, element_forces_kernel<NG, KIND, ELASTIC, M, true>));
+    else CUDA_CHECK(cudaFuncGetAttributes(&fa, element_forces_kernel<NG, KIND, ELASTIC, M, false>));
+    return;
+  }
   const int grid = ceil_div(a.blk.n, C::EPB);
   if (a.gather) {
     element_forces_kernel<NG, KIND, ELASTIC, M, true>

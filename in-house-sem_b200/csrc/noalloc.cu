@@ -12,10 +12,14 @@
 // For them, insem_cuda_solver_internal_forces_noalloc takes the field and
 // the result as device arrays the caller owns. Its one piece of scratch, the
 // element-local force vectors between the element kernels and the assembly,
-// lives in a fixed array compiled into this file. Every GPU that loads the
-// library holds that array until the process exits.
-#include <mutex>
-
+// lives in a fixed array compiled into this file.
+//
+// Under lazy module loading (the CUDA default since 12.2) the driver loads a
+// module, and reserves its device memory, the first time something in it is
+// used. Creating a solver therefore loads this file's array and the kernels
+// the entry point runs, on the solver's device (prepare_noalloc); from then
+// on that GPU holds the array until the process exits, and the entry point's
+// calls load nothing.
 #include "solver.cuh"
 
 namespace insem_b200 {
@@ -26,29 +30,35 @@ constexpr std::size_t kNoAllocScratchFloats = std::size_t{1} << 22;
 static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
 
 // In host code g_noalloc_scratch names a host-side stand-in, not device
-// memory: kernels get the device address, looked up once per device.
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-float* g_scratch_ptr[kMaxDevices] = {};
-
+// memory: kernels get the device address, looked up on the current device at
+// every call (a host-side lookup; nothing is cached, so a context that was
+// torn down and created again is addressed afresh).
 float* scratch_on_current_device() {
-  int device = 0;
-  CUDA_CHECK(cudaGetDevice(&device));
-  INSEM_REQUIRE(device >= 0 && device < kMaxDevices, INSEM_CUDA_ERR_UNSUPPORTED, "device ordinal out of range");
-  std::lock_guard<std::mutex> lk(g_scratch_mutex);
-  if (!g_scratch_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      throw Error(INSEM_CUDA_ERR_CUDA, std::string("cannot address the scratch array: ") + cudaGetErrorString(e));
-    }
-    g_scratch_ptr[device] = static_cast<float*>(p);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(INSEM_CUDA_ERR_CUDA, std::string("cannot address the scratch array: ") + cudaGetErrorString(e));
   }
-  return g_scratch_ptr[device];
+  return static_cast<float*>(p);
 }
 
 }  // namespace
+
+void Solver::prepare_noalloc() {
+  scratch_on_current_device();
+  for (const DeviceDomainData& d : domains) {
+    for (const DeviceBlock& b : d.blocks) {
+      ElementLaunch a;
+      a.blk = b.view();
+      a.gather = true;
+      a.elastic = d.medium == INSEM_ELASTIC;
+      a.preload = true;
+      launch_element_forces(ngll, a);
+    }
+    preload_assemble(d.dofs.weighted);
+  }
+}
 
 void Solver::internal_forces_noalloc(int32_t di, const float* u_global, float* f_global, cudaStream_t s) {
   INSEM_REQUIRE(di >= 0 && di < static_cast<int32_t>(domains.size()), INSEM_CUDA_ERR_INVALID, "domain out of range");

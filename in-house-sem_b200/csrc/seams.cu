@@ -71,6 +71,12 @@ void launch_gather(const DeviceDofMap& d, int ncomp, const float* global, float*
   CUDA_LAUNCH_CHECK();
 }
 
+void preload_assemble(bool weighted) {
+  cudaFuncAttributes fa;
+  if (weighted) CUDA_CHECK(cudaFuncGetAttributes(&fa, assemble_kernel<true>));
+  else CUDA_CHECK(cudaFuncGetAttributes(&fa, assemble_kernel<false>));
+}
+
 void launch_assemble(const DeviceDofMap& d, int ncomp, const float* local, float* global, cudaStream_t s) {
   if (d.n_global == 0) return;
   if (d.weighted) {

@@ -81,3 +81,29 @@ def test_noalloc_refuses_a_domain_beyond_its_scratch(pkg):
         assert b"4194304" in N.lib().insem_cuda_last_error()
         torch.cuda.synchronize()
         assert bool(torch.all(f_dev == 7.0))  # nothing was enqueued
+
+
+def test_noalloc_calls_leave_free_device_memory_unchanged(pkg):
+    """The property the entry point exists for: on a freshly created solver,
+    its first call and every later one change the device's free memory by
+    nothing (no cudaMalloc, and no module the driver loads on first use)."""
+    import torch
+
+    from insem_b200 import native as N
+
+    z = golden("bh1")  # axisymmetric m = 1: hanging-node rows, both media
+    prob = pkg.ProblemData.from_npz(z)
+    rng = np.random.default_rng(5)
+    inputs = []
+    for d in prob.domains:
+        u = torch.from_numpy(rng.uniform(-1.0, 1.0, d.ncomp * d.n_global).astype(np.float32)).cuda()
+        inputs.append((u, torch.empty_like(u)))
+    with pkg.Solver(prob) as s:
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        for _ in range(3):
+            for di, (u_dev, f_dev) in enumerate(inputs):
+                assert _noalloc(s, di, u_dev, f_dev, 0) == N.OK, N.lib().insem_cuda_last_error()
+            torch.cuda.synchronize()
+            free, _ = torch.cuda.mem_get_info()
+            assert free == free0, f"free device memory changed by {free0 - free} bytes"
