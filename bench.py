@@ -438,8 +438,11 @@ def bench_config4(args, world, rank, device, pg) -> dict:
 
 
 def bench_serving(args, device) -> dict:
-    """The serving stream through the continuous-batching server, and its first
-    part through the plain path (one solve at a time): same requests."""
+    """The serving stream through the continuous-batching server and through
+    the plain path (one solve at a time), on the same requests, at each
+    arrival rate of --serve-rates (rates one GPU sustains, so latency is
+    service time plus short queueing) and at --serve-rate (the stated 50/s,
+    above one GPU's capacity: latency there is mostly queueing)."""
     import __graft_entry__ as entry
 
     entry.load_package()
@@ -448,22 +451,29 @@ def bench_serving(args, device) -> dict:
     # warm-up: a short stream of the same mix loads the kernels every class uses
     S.Server(device=device, chunk_steps=args.serve_chunk).run(
         S.request_stream(rate=200.0, window=1.0, seed=55, time_scale=1e-3, max_requests=24), keep_traces=False)
-    stream = S.request_stream(rate=args.serve_rate, window=args.serve_window, time_scale=args.serve_scale)
-    t0 = time.perf_counter()
-    batched = S.summarize(S.Server(device=device, chunk_steps=args.serve_chunk).run(stream, keep_traces=False))
-    wall_b = time.perf_counter() - t0
-    sub = stream[: max(1, int(len(stream) * args.serve_plain_fraction))]
-    t0 = time.perf_counter()
-    plain = S.summarize(S.serve_plain(sub, device=device))
-    wall_p = time.perf_counter() - t0
-    out = {"workload": f"Poisson {args.serve_rate:g}/s over {args.serve_window:g} s: 40 % Cartesian (2k-200k "
-                       f"elements, order 3-8), 35 % monopole and 25 % dipole boreholes from the batched set; "
-                       f"simulated durations U(2, 8) ms x {args.serve_scale:g}",
-           "batched": batched, "plain": plain, "plain_requests": len(sub),
-           "wall_seconds": {"batched": round(wall_b, 1), "plain": round(wall_p, 1)}}
-    if batched.get("value") and plain.get("value"):
-        out["batched_over_plain"] = batched["value"] / plain["value"]
-    return out
+
+    def point(rate: float, window: float, seed: int) -> dict:
+        stream = S.request_stream(rate=rate, window=window, seed=seed, time_scale=args.serve_scale)
+        t0 = time.perf_counter()
+        batched = S.summarize(S.Server(device=device, chunk_steps=args.serve_chunk).run(stream, keep_traces=False))
+        wall_b = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        plain = S.summarize(S.serve_plain(stream, device=device))
+        wall_p = time.perf_counter() - t0
+        out = {"rate_per_s": rate, "window_s": window, "requests": len(stream), "batched": batched, "plain": plain,
+               "wall_seconds": {"batched": round(wall_b, 1), "plain": round(wall_p, 1)}}
+        if batched.get("value") and plain.get("value"):
+            out["batched_over_plain"] = batched["value"] / plain["value"]
+        return out
+
+    rates = [float(x) for x in args.serve_rates.split(",") if x.strip()] if args.serve_rates else []
+    points = [point(r, args.serve_window_sustained, 5 + i) for i, r in enumerate(rates)]
+    overload = point(args.serve_rate, args.serve_window, 5)
+    return {"workload": "Poisson arrivals: 40 % Cartesian (2k-200k elements, order 3-8), 35 % monopole and 25 % "
+                        f"dipole boreholes from the batched set; simulated durations U(2, 8) ms x {args.serve_scale:g}; "
+                        "the batched and the plain server serve the same requests at each rate",
+            "sustained": points, "overload": overload,
+            "batched_over_plain": overload.get("batched_over_plain")}
 
 
 def run_ours(args, world, rank, local, pg):
@@ -525,11 +535,13 @@ def main():
                     help="batched workload: host threads building the models and their stable time steps")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving: mean arrivals per second")
-    ap.add_argument("--serve-window", type=float, default=4.0, help="serving: seconds of arrivals")
+    ap.add_argument("--serve-window", type=float, default=3.0, help="serving: seconds of arrivals at --serve-rate")
+    ap.add_argument("--serve-rates", default="2,4",
+                    help="serving: arrival rates (per s) one GPU sustains, measured besides --serve-rate")
+    ap.add_argument("--serve-window-sustained", type=float, default=8.0,
+                    help="serving: seconds of arrivals at each of --serve-rates")
     ap.add_argument("--serve-scale", type=float, default=0.25, help="serving: factor on the simulated durations")
     ap.add_argument("--serve-chunk", type=int, default=64, help="serving: batched steps between admissions")
-    ap.add_argument("--serve-plain-fraction", type=float, default=0.25,
-                    help="serving: share of the stream (from its start) also served by the plain path")
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the streamed end-to-end run")

@@ -44,7 +44,7 @@ def units() -> list[tuple[Path, list[str], Path]]:
     for ng in range(2, 10):
         out.append((CSRC / "element_ng.cu", [f"-DINSEM_NG={ng}"], OBJ / f"element_ng{ng}.o"))
         out.append((CSRC / "tiled_ng.cu", [f"-DINSEM_NG={ng}"], OBJ / f"tiled_ng{ng}.o"))
-    for name in ("seams.cu", "solver.cu", "tiled_path.cu", "batch.cu", "noalloc.cu"):
+    for name in ("seams.cu", "solver.cu", "tiled_path.cu", "batch.cu", "snapshots.cu", "noalloc.cu"):
         if (CSRC / name).exists():
             out.append((CSRC / name, [], OBJ / (Path(name).stem + ".o")))
     return out

@@ -283,6 +283,8 @@ class Model:
     safety: float = 0.8
     record_every: int = 1
     energy_every: int = 0
+    snapshot_every: int = 0  # wavefield snapshots (Solver.set_snapshots), 0 = off
+    snapshot_quantities: Tuple[str, ...] = ("velocity", "pressure")
 
 
 _cases_lib = None

@@ -34,6 +34,7 @@ static __global__ void batch_row_gather_kernel(const StreamSeg* __restrict__ seg
 void Solver::batch_prepare() {
   DeviceGuard dg(device);
   INSEM_REQUIRE(tiled, INSEM_CUDA_ERR_STATE, "batched solves run on the tiled path");
+  INSEM_REQUIRE(snap_every <= 0, INSEM_CUDA_ERR_STATE, "a solve that records snapshots is stepped on its own");
   if (in_batch) return;  // prepared already
   if (!initialized) {
     set_mode(kModeInit);
@@ -186,6 +187,7 @@ void Solver::check_fields() {
   StepState hs;
   CUDA_CHECK(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, stream));
   CUDA_CHECK(cudaStreamSynchronize(stream));
+  if (hs.nonfinite) nonfinite_seen = true;
   INSEM_REQUIRE(!hs.nonfinite, INSEM_CUDA_ERR_NONFINITE, "the solution contains NaN or Inf (unstable time step?)");
 }
 
@@ -453,7 +455,7 @@ int32_t Batch::max_remaining() const {
 // After k batched steps: each running solve did min(k, its remaining) steps
 // and idled after its last one.
 void Batch::credit(int32_t k) {
-  std::vector<Solver*> done;
+  std::vector<std::pair<std::size_t, Solver*>> done;
   for (std::size_t i = 0; i < members.size(); ++i) {
     if (!members[i] || !prepared[i] || members[i]->s->remaining() <= 0) continue;
     Solver& s = *members[i]->s;
@@ -462,12 +464,24 @@ void Batch::credit(int32_t k) {
     point_updates += member_points[i] * d;
     if (s.remaining() == 0) {
       dirty = true;
-      done.push_back(&s);
+      done.push_back({i, &s});
     }
   }
   INSEM_REQUIRE(!*herr, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
-  if (opts.check_finite)
-    for (Solver* s : done) s->check_fields();
+  if (!opts.check_finite) return;
+  // every member that finished is checked; the error names all that failed
+  // (each is marked: insem_cuda_solver_status), the others are complete
+  std::string failed;
+  for (const auto& [i, s] : done) {
+    try {
+      s->check_fields();
+    } catch (const Error& e) {
+      if (e.code != INSEM_CUDA_ERR_NONFINITE) throw;
+      failed += (failed.empty() ? "" : ", ") + std::to_string(i);
+    }
+  }
+  INSEM_REQUIRE(failed.empty(), INSEM_CUDA_ERR_NONFINITE,
+                "batch members " + failed + ": the solution contains NaN or Inf (unstable time step?)");
 }
 
 void Batch::finish_steps() {

@@ -173,6 +173,7 @@ Solver::Solver(const insem_cuda_problem& p, const insem_cuda_options* opt, bool 
   if (setup_only || opts.path == 1)
     for (auto& d : domains) d.alloc_fields();
   if (!setup_only && opts.path != 1) build_tiled(p);
+  if (!setup_only) prepare_noalloc();
   // uploads and zeroing ran on the legacy stream and this solver's stream;
   // other streams (other solvers, batches) are not waited for
   CUDA_CHECK(cudaStreamSynchronize(nullptr));
@@ -681,6 +682,29 @@ void Solver::advance(int32_t n) {
   DeviceGuard dg(device);
   INSEM_REQUIRE(n >= 0, INSEM_CUDA_ERR_INVALID, "negative step count");
   INSEM_REQUIRE(!in_batch, INSEM_CUDA_ERR_STATE, "this solve is stepped by a batch");
+  if (snap_every <= 0) {
+    advance_span(n);
+    return;
+  }
+  // spans that end on snapshot steps, where the state is complete
+  double ms = 0.0;
+  if (!initialized) {
+    advance_span(0);
+    ms += last_ms;
+    record_snapshot();
+  }
+  int32_t left = std::min<int32_t>(n, n_steps - step);
+  while (left > 0) {
+    const int32_t k = std::min<int32_t>(left, snap_every - step % snap_every);
+    advance_span(k);
+    ms += last_ms;
+    left -= k;
+    if (step % snap_every == 0) record_snapshot();
+  }
+  last_ms = ms;
+}
+
+void Solver::advance_span(int32_t n) {
   if (tiled) {
     int32_t dummy = 0;
     advance_tiled(n, nullptr, nullptr, &dummy);
@@ -713,6 +737,7 @@ void Solver::advance(int32_t n) {
   if (opts.check_finite) {
     StepState hs;
     CUDA_CHECK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
+    if (hs.nonfinite) nonfinite_seen = true;
     INSEM_REQUIRE(!hs.nonfinite, INSEM_CUDA_ERR_NONFINITE, "the solution contains NaN or Inf (unstable time step?)");
   }
 }
@@ -747,6 +772,7 @@ void Solver::ensure_graph() {
 // Per step: source amplitudes in (H2D), the step's graph, the record row out (D2H).
 void Solver::advance_streamed(int32_t n, const float* amp_in, double* rows_out, int32_t* n_rows) {
   INSEM_REQUIRE(!in_batch, INSEM_CUDA_ERR_STATE, "this solve is stepped by a batch");
+  INSEM_REQUIRE(snap_every <= 0, INSEM_CUDA_ERR_STATE, "snapshots are recorded by advance(), not the streamed form");
   DeviceGuard dg(device);
   INSEM_REQUIRE(n >= 0 && n_rows, INSEM_CUDA_ERR_INVALID, "invalid streamed advance");
   INSEM_REQUIRE(n_sources == 0 || amp_in, INSEM_CUDA_ERR_INVALID, "missing source amplitudes");
@@ -1129,6 +1155,7 @@ void Solver::advance_tiled(int32_t n, const float* amp_in, double* rows_out, int
   StepState hs;
   CUDA_CHECK(cudaMemcpy(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost));
   INSEM_REQUIRE(!hs.error, INSEM_CUDA_ERR_TIMEOUT, "a tile's bulk copies did not arrive within the wait limit");
+  if (hs.nonfinite) nonfinite_seen = true;
   if (opts.check_finite && !streamed)
     INSEM_REQUIRE(!hs.nonfinite, INSEM_CUDA_ERR_NONFINITE, "the solution contains NaN or Inf (unstable time step?)");
 }
@@ -1186,6 +1213,10 @@ int insem_cuda_solver_run(insem_cuda_solver* h) {
 }
 
 int32_t insem_cuda_solver_step(const insem_cuda_solver* h) { return h ? h->s->step : -1; }
+int32_t insem_cuda_solver_status(const insem_cuda_solver* h) {
+  if (!h) return INSEM_CUDA_ERR_INVALID;
+  return h->s->nonfinite_seen ? INSEM_CUDA_ERR_NONFINITE : INSEM_CUDA_OK;
+}
 int32_t insem_cuda_solver_n_steps(const insem_cuda_solver* h) { return h ? h->s->n_steps : -1; }
 double insem_cuda_solver_dt(const insem_cuda_solver* h) { return h ? h->s->dt : 0.0; }
 int32_t insem_cuda_solver_n_samples(const insem_cuda_solver* h) { return h ? h->s->n_samples() : -1; }

@@ -60,6 +60,17 @@ class Solver {
 
   void set_state(int32_t medium, const double* u, const double* v);
   void advance(int32_t n);
+  // Wavefield snapshots (Solver::record_snapshot, solver.cpp:813-839): every
+  // `every` steps (and at step 0) the listed quantities of every medium that
+  // has them, gathered to element points.  Before the first step only.
+  void set_snapshots(int32_t every, int32_t n_quantities, const int32_t* quantities);
+  struct SnapField {
+    int32_t domain = 0, quantity = 0, ncomp = 0;
+    std::vector<float> data;  // [snapshot][component][element * npe + k]
+  };
+  int32_t snap_every = 0;
+  std::vector<SnapField> snap_fields;
+  std::vector<double> snap_times;
   void advance_streamed(int32_t n, const float* amp_in, double* rows_out, int32_t* n_rows);
   void ensure_graph();
   int32_t kernels_per_step = 0;
@@ -75,6 +86,10 @@ class Solver {
   // f = -K u of domain di on the caller's device arrays, without allocating
   // (the element-local forces use a fixed array, see noalloc.cu).
   void internal_forces_noalloc(int32_t di, const float* u_global, float* f_global, cudaStream_t s);
+  // Run by the constructor on the solver's device: loads the fixed scratch
+  // array and the kernels internal_forces_noalloc launches, so that under lazy
+  // module loading none of them is loaded (allocated) by a later call.
+  void prepare_noalloc();
 
   insem_cuda_options opts{};
   int device = 0;
@@ -83,6 +98,11 @@ class Solver {
   double stable_dt_estimate = 0.0;  // set by the timed constructor
   int32_t n_steps = 0, step = 0, record_every = 1, energy_every = 0;
   bool initialized = false;
+  std::vector<DeviceBuffer<int32_t>> snap_l2g;  // per domain: element slot -> field point, or -1 - constraint row
+  DeviceBuffer<float> snap_stage;
+  void record_snapshot();
+  void advance_span(int32_t n);
+  bool nonfinite_seen = false;  // a finite check found NaN or Inf in the fields
   double last_ms = 0.0;
   cudaStream_t stream = nullptr;
   std::vector<DeviceDomainData> domains;

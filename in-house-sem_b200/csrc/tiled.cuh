@@ -206,13 +206,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 constexpr uint32_t kBulkWaitLimit = 1u << 22;
 
 // Shared-memory layout of one tile CTA, byte offsets (16-byte aligned).
-// Per-tile data arrives by bulk copies: element data (metric, coefficients,
-// axisymmetric weights), slot descriptors, and the complete points' u, v
-// and inverse mass (v and 1/M later, when `late`); halo tile points are
-// gathered by the threads into the u region after the complete points (at
-// index roundup(nc, 4) on).
+// Per-tile data arrives by bulk copies: element data (metric, axisymmetric
+// weights), slot descriptors, and the complete points' u, v and inverse mass
+// (v and 1/M later, when `late`); halo tile points are gathered by the
+// threads into the u region after the complete points (at index
+// roundup(nc, 4) on).  The material coefficients (one pair per element) and
+// the slot descriptors (which each column thread keeps in registers) are read
+// from global memory by the threads that use them.
 struct TileLayout {
-  uint32_t bar, metric, coef0, coef1, wr, hoop, r, desc, u, v, im, tf, su, sfx, ax, total;
+  uint32_t bar, metric, wr, hoop, r, u, v, im, tf, su, sfx, ax, total;
   int32_t tp_cap, nc_cap, ms, cs, row;
   int32_t late;  // 1: v and 1/M arrive by a second copy into the element-data region
 
@@ -231,18 +233,12 @@ struct TileLayout {
     o = up16(o + 16);
     L.metric = o;
     o = up16(o + 4u * te * L.ms);
-    L.coef0 = o;
-    o = up16(o + 4u * te * L.cs);
-    L.coef1 = o;
-    if (elastic) o = up16(o + 4u * te * L.cs);
     L.wr = o;
     if (axi) o = up16(o + 4u * te * L.cs);
     L.hoop = o;
     if (axi) o = up16(o + 4u * te * L.cs);
     L.r = o;
     if (axi) o = up16(o + 4u * te * L.cs);
-    L.desc = o;
-    o = up16(o + 4u * te * L.cs);
     // The element data [metric, elem_end) is last read by the fluxes.  The
     // f_xi rows (written after the fluxes, read by the divergence) and then
     // the assembly target with v and 1/M (copied in after the divergence)
@@ -348,12 +344,9 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   constexpr bool AXI = KIND == INSEM_AXISYM;
   constexpr int MS = KIND == INSEM_RECT ? 4 : KIND == INSEM_AFFINE ? 8 : (AXI ? 4 : 5) * CS;
   float* s_metric = reinterpret_cast<float*>(smem_raw + L.metric);
-  float* s_coef0 = reinterpret_cast<float*>(smem_raw + L.coef0);
-  float* s_coef1 = reinterpret_cast<float*>(smem_raw + L.coef1);
   float* s_wr = reinterpret_cast<float*>(smem_raw + L.wr);
   float* s_hoop = reinterpret_cast<float*>(smem_raw + L.hoop);
   float* s_r = reinterpret_cast<float*>(smem_raw + L.r);
-  uint32_t* s_desc = reinterpret_cast<uint32_t*>(smem_raw + L.desc);
   float* tu = reinterpret_cast<float*>(smem_raw + L.u);    // [NC][tp_cap]
   float* s_v = reinterpret_cast<float*>(smem_raw + L.v);   // [NC][nc_cap]
   float* s_im = reinterpret_cast<float*>(smem_raw + L.im); // [nc_cap]
@@ -375,19 +368,16 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   //    points (u; v and 1/M too unless they come late)
   if (tid == 0) {
     const uint32_t eb = 4u * th.ne;
-    uint32_t total = eb * MS + eb * CS * (1 + (EL ? 1 : 0) + (AXI ? 3 : 0)) + eb * CS;
+    uint32_t total = eb * MS + eb * CS * (AXI ? 3 : 0);
     if (nc4 > 0) total += 4u * nc4 * (L.late ? NC : 2 * NC + 1);
     fence_proxy_async_smem();
     mbar_expect_tx(bar, total);
     bulk_load(s_metric, blk.metric + static_cast<size_t>(th.be0) * MS, eb * MS, bar);
-    bulk_load(s_coef0, blk.coef0 + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
-    if constexpr (EL) bulk_load(s_coef1, blk.coef1 + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
     if constexpr (AXI) {
       bulk_load(s_wr, blk.wr + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
       bulk_load(s_hoop, blk.hoop + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
       bulk_load(s_r, blk.r + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
     }
-    bulk_load(s_desc, td.sdesc + static_cast<size_t>(th.be0) * CS, eb * CS, bar);
     if (nc4 > 0) {
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
@@ -396,6 +386,16 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       }
       if (!L.late) bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar);
     }
+  }
+  // this column's slot descriptors, loaded while the bulk copies are in flight
+  const int el = tid / NG;
+  const int i = tid - el * NG;
+  const bool active = el < th.ne;
+  uint32_t dsc[NG];
+  if (active) {
+    const uint32_t* gdesc = td.sdesc + static_cast<size_t>(th.be0 + el) * CS + i;
+#pragma unroll
+    for (int j = 0; j < NG; ++j) dsc[j] = gdesc[j * NG];
   }
   // halo tile points, gathered while the bulk copies are in flight
   for (int t = tid; t < th.ntp - th.nc; t += nthreads) {
@@ -411,19 +411,16 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     return false;
   }
 
-  // element data now in shared memory, indexed by the tile-local element
+  // element data now in shared memory, indexed by the tile-local element;
+  // the coefficients (one pair per element) stay in global memory
   BlockDev lb = blk;
   lb.metric = s_metric;
-  lb.coef0 = s_coef0;
-  lb.coef1 = s_coef1;
+  lb.coef0 = blk.coef0 + th.be0;
+  lb.coef1 = EL ? blk.coef1 + th.be0 : nullptr;
   lb.wr = s_wr;
   lb.hoop = s_hoop;
   lb.r = s_r;
 
-  const int el = tid / NG;
-  const int i = tid - el * NG;
-  const bool active = el < th.ne;
-  const uint32_t* desc = s_desc + el * CS;
   constexpr int ES = rows_elem_stride(NG, NC);  // element stride of the rows
   constexpr bool PAIR = NC == 2;                 // interleaved components, two-lane sums
   // position of (component c, row j, column l) in an element's rows
@@ -434,11 +431,9 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   float* ax = sax + el * 4 * AXS;
 
   // 2. element field rows (slots through their tile point or the constrained list)
-  uint32_t dsc[NG];
   if (active) {
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
-      dsc[j] = desc[j * NG + i];
       if (!(dsc[j] & kSlotConstrained)) {
         const int p = dsc[j] & kSlotPointMask;
         if constexpr (PAIR) {
@@ -499,7 +494,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
         const float2 av = upk2(a), bv = upk2(b);
         float uxi[NC] = {av.x, av.y}, ueta[NC] = {bv.x, bv.y}, upt[NC] = {ucol[0][j], ucol[1][j]};
         float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f};
-        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
+        point_flux<NG, KIND, EL, M, true>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
                                     ax + 3 * AXS, w2c[j]);
         fx[0][j] = fxp[0];
         fx[1][j] = fxp[1];
@@ -532,7 +527,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
         float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f}, upt[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
-        point_flux<NG, KIND, EL, M>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
+        point_flux<NG, KIND, EL, M, true>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
                                     ax + 3 * AXS, w2c[j]);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {

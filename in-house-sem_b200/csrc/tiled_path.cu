@@ -16,6 +16,7 @@
 //      through a CSR in ascending slot order (weights of constrained maps kept).
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <numeric>
@@ -188,6 +189,14 @@ int tile_batch(int ngll, const TileBatchLaunch& a, bool launch) {
   }
   return 0;
 }
+
+namespace {
+uint32_t bits_of(float v) {
+  uint32_t b;
+  std::memcpy(&b, &v, sizeof b);
+  return b;
+}
+}  // namespace
 
 BlockDev TiledDomain::BlockTiles::view() const {
   BlockDev v;
@@ -579,8 +588,23 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
       for (int32_t e : tile_elems[t]) order.push_back(epos[e]);
     PackedBlock pk = pack_block(d.blocks[b], npe, medium, order);
     blocks[b].metric.upload(pk.metric);
-    blocks[b].coef0.upload(pk.coef0);
-    if (medium == INSEM_ELASTIC) blocks[b].coef1.upload(pk.coef1);
+    // One material per element: the tile kernels read one coefficient pair
+    // per element instead of one per point.
+    const std::size_t cs = point_stride_rt(npe);
+    std::vector<float> c0(order.size()), c1(medium == INSEM_ELASTIC ? order.size() : 0);
+    for (std::size_t q = 0; q < order.size(); ++q) {
+      c0[q] = pk.coef0[q * cs];
+      if (!c1.empty()) c1[q] = pk.coef1[q * cs];
+      for (int k = 1; k < npe; ++k) {
+        const bool same = bits_of(pk.coef0[q * cs + k]) == bits_of(c0[q]) &&
+                          (c1.empty() || bits_of(pk.coef1[q * cs + k]) == bits_of(c1[q]));
+        INSEM_REQUIRE(same, INSEM_CUDA_ERR_UNSUPPORTED,
+                      "material coefficients vary inside an element; the tiled path takes one material per "
+                      "element (options.path = 1 takes per-point coefficients)");
+      }
+    }
+    blocks[b].coef0.upload(c0);
+    if (medium == INSEM_ELASTIC) blocks[b].coef1.upload(c1);
     if (d.blocks[b].kind == INSEM_AXISYM) {
       blocks[b].wr.upload(pk.wr);
       blocks[b].hoop.upload(pk.hoop);

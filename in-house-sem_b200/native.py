@@ -132,6 +132,7 @@ def lib() -> C.CDLL:
             "insem_cuda_solver_advance": (C.c_int, [vp, C.c_int32]),
             "insem_cuda_solver_run": (C.c_int, [vp]),
             "insem_cuda_solver_step": (C.c_int32, [vp]),
+            "insem_cuda_solver_status": (C.c_int32, [vp]),
             "insem_cuda_solver_n_steps": (C.c_int32, [vp]),
             "insem_cuda_solver_dt": (C.c_double, [vp]),
             "insem_cuda_solver_n_samples": (C.c_int32, [vp]),
@@ -141,6 +142,12 @@ def lib() -> C.CDLL:
             "insem_cuda_solver_times": (C.c_int, [vp, f64p]),
             "insem_cuda_solver_energy": (C.c_int, [vp, f64p, C.c_int32, i32p]),
             "insem_cuda_solver_state": (C.c_int, [vp, C.c_int32, f64p, f64p, f64p]),
+            "insem_cuda_solver_set_snapshots": (C.c_int, [vp, C.c_int32, C.c_int32, i32p]),
+            "insem_cuda_solver_n_snapshots": (C.c_int32, [vp]),
+            "insem_cuda_solver_n_snapshot_fields": (C.c_int32, [vp]),
+            "insem_cuda_solver_snapshot_field": (C.c_int, [vp, C.c_int32, i32p, i32p, i32p, C.POINTER(C.c_int64)]),
+            "insem_cuda_solver_snapshot": (C.c_int, [vp, C.c_int32, f32p]),
+            "insem_cuda_solver_snapshot_times": (C.c_int, [vp, f64p]),
             "insem_cuda_solver_last_advance_ms": (C.c_double, [vp]),
             "insem_cuda_solver_internal_forces": (C.c_int, [vp, C.c_int32, f32p, f32p]),
             "insem_cuda_solver_internal_forces_noalloc": (C.c_int, [vp, C.c_int32, vp, vp, vp]),

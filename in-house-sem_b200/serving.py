@@ -22,6 +22,14 @@ time, each with its own step graphs, in arrival order.
 Batching does not change results: each request's traces and fields are those
 it gets alone, bit for bit (tests/test_gpu_serving.py).
 
+Failures stay with the request that caused them.  A request whose setup
+fails (a source outside its medium, an unknown material region, ...), whose
+device set-up fails, or whose footprint exceeds the whole HBM budget is
+marked failed or rejected, with the error, and the stream goes on.  A batch
+member whose fields turn non-finite is found when its last step runs, marked
+failed and evicted; the members stepping beside it are unaffected (their
+arrays are their own) and complete normally.
+
 The reference has no serving loop. Its hook for one is one ``Simulation``
 per thread (python/src/bindings.cpp:336-337).
 """
@@ -33,7 +41,7 @@ from collections import deque
 from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 from dataclasses import dataclass
-from typing import Dict, List, Optional
+from typing import Callable, Dict, List, Optional
 
 import numpy as np
 
@@ -52,6 +60,9 @@ class Request:
     arrival: float          # seconds after the stream starts
     kind: str
     spec: dict
+    # Optional initial state: called with the new solver before its first
+    # step (for Solver.set_state, as with the reference's set_state).
+    init: Optional[Callable] = None
 
 
 @dataclass
@@ -67,6 +78,8 @@ class Record:
     elements: int = 0
     device_bytes: int = 0
     traces: Optional[np.ndarray] = None  # [n_samples][columns], streamed
+    status: str = "pending"  # "done", "failed" (error says why) or "rejected" (over the HBM budget)
+    error: str = ""
 
 
 # ---------------------------------------------------------------- workload
@@ -180,12 +193,19 @@ def _stage_host(req: Request):
     return model, arrays, ne, device_bytes_estimate(ProblemData.from_npz(probe))
 
 
-def _stage_device(model, arrays, device: int, use_graphs: bool, prepare: bool):
-    """Stage B (device, worker thread): dt from the power iteration, the solver
-    (and, for the batched server, its initial step and predictor)."""
+def _stage_device(model, arrays, device: int, use_graphs: bool, prepare: bool, init=None):
+    """Stage B (device, worker thread): dt from the power iteration, the solver,
+    the request's initial state (and, for the batched server, its initial step
+    and predictor)."""
     prob, s = K.build_solver_from_arrays(model, arrays, device=device, use_graphs=use_graphs)
-    if prepare:
-        s.prepare_for_batch()
+    try:
+        if init is not None:
+            init(s)
+        if prepare:
+            s.prepare_for_batch()
+    except Exception:
+        s.close()
+        raise
     return prob, s
 
 
@@ -204,6 +224,7 @@ class _Pipeline:
         self.dev: deque = deque()            # (rid, bytes, future of stage B), admission order
         self.used = 0
         self.i = 0
+        self.stream_by_rid = {r.rid: r for r in stream}
         self.t0 = time.perf_counter()
 
     def now(self) -> float:
@@ -212,8 +233,14 @@ class _Pipeline:
     def pending(self) -> bool:
         return self.i < len(self.stream) or bool(self.host) or bool(self.waiting) or bool(self.dev)
 
+    def fail(self, rid: int, error: Exception, status: str = "failed") -> None:
+        rec = self.recs[rid]
+        rec.status, rec.error, rec.completed = status, f"{type(error).__name__}: {error}", float("nan")
+
     def poll(self, running: int) -> List[tuple]:
-        """Advances the pipeline; returns (rid, problem, solver, bytes) now ready."""
+        """Advances the pipeline; returns (rid, problem, solver, bytes) now ready.
+        Requests whose setup fails, or that could never fit the budget, leave
+        the pipeline marked failed or rejected."""
         now = self.now()
         while self.i < len(self.stream) and self.stream[self.i].arrival <= now:
             r = self.stream[self.i]
@@ -223,11 +250,19 @@ class _Pipeline:
             f = self.host[rid]
             if not f.done():
                 break  # keep arrival order
-            model, arrays, ne, need = f.result()
+            del self.host[rid]
+            try:
+                model, arrays, ne, need = f.result()
+            except Exception as e:  # the request's own setup failed
+                self.fail(rid, e)
+                continue
             rec = self.recs[rid]
             rec.setup_done, rec.elements, rec.device_bytes = self.now(), ne, need
+            if need > self.budget:
+                self.fail(rid, MemoryError(f"needs {need} bytes of device memory, the budget is {self.budget}"),
+                          "rejected")
+                continue
             self.waiting.append((rid, model, arrays, need))
-            del self.host[rid]
         while self.waiting:
             rid, model, arrays, need = self.waiting[0]
             if (running or self.dev) and self.used + need > self.budget:
@@ -236,11 +271,17 @@ class _Pipeline:
             self.used += need
             self.recs[rid].admitted = self.now()
             self.dev.append((rid, need, self.pool.submit(_stage_device, model, arrays, self.device,
-                                                         self.use_graphs, self.prepare)))
+                                                         self.use_graphs, self.prepare,
+                                                         self.stream_by_rid[rid].init)))
         out = []
         while self.dev and self.dev[0][2].done():
             rid, need, f = self.dev.popleft()
-            prob, solver = f.result()
+            try:
+                prob, solver = f.result()
+            except Exception as e:  # device set-up of this request failed
+                self.release(need)
+                self.fail(rid, e)
+                continue
             rec = self.recs[rid]
             rec.points, rec.steps = prob.n_global_total(), prob.n_steps
             out.append((rid, prob, solver, need))
@@ -308,7 +349,14 @@ class Server:
                 left = {m.index: m.n_steps - m.step for m in act}
                 _, row_cols = batch.stream_layout()
                 rows = np.empty((self.chunk, max(row_cols, 1)))
-                done = batch.advance_streamed(self.chunk, None, rows)
+                try:
+                    done = batch.advance_streamed(self.chunk, None, rows)
+                except N.InsemError as e:
+                    if e.code != N.ERR_NONFINITE:
+                        raise
+                    # the steps ran and the rows are in; the members that
+                    # failed are marked and leave below
+                    done = min(self.chunk, max(left.values()))
                 col = 0
                 for m in act:
                     nc = m.n_columns
@@ -318,7 +366,12 @@ class Server:
                 for idx in [j for j, (_, m, _, _) in members.items() if m.step >= m.n_steps]:
                     rid, m, need, blocks = members.pop(idx)
                     r = recs[rid]
-                    r.completed = pipe.now()
+                    if m.failed:
+                        pipe.fail(rid, N.InsemError(N.ERR_NONFINITE, "the solution contains NaN or Inf"))
+                        batch.remove(m)
+                        pipe.release(need)
+                        continue
+                    r.completed, r.status = pipe.now(), "done"
                     if keep_traces:
                         n_tr = len(m.problem.trace_list())
                         first = (np.concatenate([m.trace_by_index(t)[:1] for t in range(n_tr)], axis=1)
@@ -354,12 +407,19 @@ def serve_plain(stream: List[Request], device: int = 0, workers: Optional[int] =
                 continue
             rid, prob, s, need = ready.popleft()
             with s:
-                s.run()
+                try:
+                    s.run()
+                except N.InsemError as e:
+                    if e.code != N.ERR_NONFINITE:
+                        raise
+                    pipe.fail(rid, e)
+                    pipe.release(need)
+                    continue
                 if keep_traces:
                     n_tr = len(prob.trace_list())
                     recs[rid].traces = (np.concatenate([s.trace_by_index(t) for t in range(n_tr)], axis=1)
                                         if n_tr else np.zeros((prob.n_steps + 1, 0)))
-            recs[rid].completed = pipe.now()
+            recs[rid].completed, recs[rid].status = pipe.now(), "done"
             pipe.release(need)
     finally:
         pipe.close()
@@ -368,14 +428,16 @@ def serve_plain(stream: List[Request], device: int = 0, workers: Optional[int] =
 
 def summarize(recs: Dict[int, Record]) -> dict:
     """p50/p99 latency (from admission and from arrival) and aggregate throughput."""
-    done = [r for r in recs.values() if np.isfinite(r.completed)]
+    done = [r for r in recs.values() if r.status == "done"]
+    failed = sum(r.status == "failed" for r in recs.values())
+    rejected = sum(r.status == "rejected" for r in recs.values())
     if not done:
-        return {"completed": 0, "requests": len(recs)}
+        return {"completed": 0, "requests": len(recs), "failed": failed, "rejected": rejected}
     lat_adm = np.array([r.completed - r.admitted for r in done])
     lat_arr = np.array([r.completed - r.arrival for r in done])
     span = max(r.completed for r in done) - min(r.arrival for r in done)
     updates = sum(r.points * r.steps for r in done)
-    return {"completed": len(done), "requests": len(recs),
+    return {"completed": len(done), "requests": len(recs), "failed": failed, "rejected": rejected,
             "p50_ms_from_admission": 1e3 * float(np.percentile(lat_adm, 50)),
             "p99_ms_from_admission": 1e3 * float(np.percentile(lat_adm, 99)),
             "p50_ms_from_arrival": 1e3 * float(np.percentile(lat_arr, 50)),

@@ -72,6 +72,11 @@ class Solver:
         return int(N.lib().insem_cuda_solver_step(self._h))
 
     @property
+    def failed(self) -> bool:
+        """A finite check found NaN or Inf in this solve's fields."""
+        return int(N.lib().insem_cuda_solver_status(self._h)) == N.ERR_NONFINITE
+
+    @property
     def time(self) -> float:
         return self.step * self.dt
 
@@ -185,6 +190,35 @@ class Solver:
         if n.value:
             N.check(N.lib().insem_cuda_solver_energy(self._h, out.ctypes.data_as(N.f64p), n.value, C.byref(n)))
         return out
+
+    # --------------------------------------------------------- snapshots
+    def set_snapshots(self, every: int, quantities=("velocity", "pressure")) -> None:
+        """Wavefield snapshots every `every` steps and at step 0 (the
+        reference's TimeConfig snapshot_every / snapshot_quantities); before
+        the first step."""
+        q = np.ascontiguousarray([N.QUANTITIES[x] for x in quantities], np.int32)
+        N.check(N.lib().insem_cuda_solver_set_snapshots(self._h, int(every), int(q.size), q.ctypes.data_as(N.i32p)))
+
+    @property
+    def snapshot_times(self) -> np.ndarray:
+        out = np.empty(int(N.lib().insem_cuda_solver_n_snapshots(self._h)))
+        N.check(N.lib().insem_cuda_solver_snapshot_times(self._h, out.ctypes.data_as(N.f64p)))
+        return out
+
+    def snapshot(self, medium: str, quantity: str) -> np.ndarray:
+        """(n_snapshots, ncomp, n_points) snapshot data, as the reference's Solver.snapshot."""
+        want = (N.ACOUSTIC if medium == "acoustic" else N.ELASTIC, N.QUANTITIES[quantity])
+        for f in range(int(N.lib().insem_cuda_solver_n_snapshot_fields(self._h))):
+            med, qu, nc, npts = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int64()
+            N.check(N.lib().insem_cuda_solver_snapshot_field(self._h, f, C.byref(med), C.byref(qu), C.byref(nc),
+                                                             C.byref(npts)))
+            if (med.value, qu.value) != want:
+                continue
+            ns = int(N.lib().insem_cuda_solver_n_snapshots(self._h))
+            out = np.empty((ns, nc.value, npts.value), np.float32)
+            N.check(N.lib().insem_cuda_solver_snapshot(self._h, f, out.ctypes.data_as(N.f32p)))
+            return out
+        raise N.InsemError(N.ERR_INVALID, f"no {quantity} snapshots for the {medium} medium")
 
     def internal_forces(self, domain: int, u: np.ndarray) -> np.ndarray:
         d = self.problem.domains[domain]

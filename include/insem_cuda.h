@@ -285,6 +285,12 @@ int insem_cuda_solver_advance(insem_cuda_solver* h, int32_t n);
 /* Advances to the end (Solver::run). */
 int insem_cuda_solver_run(insem_cuda_solver* h);
 int32_t insem_cuda_solver_step(const insem_cuda_solver* h);
+/* INSEM_CUDA_ERR_NONFINITE once a finite check of this solve (the end of an
+ * advance, or a batch member's last step) found NaN or Inf in its fields,
+ * else INSEM_CUDA_OK.  A batch advance that fails this way names the members
+ * in its message; this tells a server which of them to evict.  No reference
+ * counterpart (the reference raises from Solver::advance). */
+int32_t insem_cuda_solver_status(const insem_cuda_solver* h);
 int32_t insem_cuda_solver_n_steps(const insem_cuda_solver* h);
 double insem_cuda_solver_dt(const insem_cuda_solver* h);
 /* Number of recorded samples so far, traces and their component counts. */
@@ -297,6 +303,26 @@ int insem_cuda_solver_trace(insem_cuda_solver* h, int32_t trace, double* out);
 int insem_cuda_solver_times(insem_cuda_solver* h, double* out);
 /* Energy samples ([n][3]: time, kinetic, potential); *n_out receives n. */
 int insem_cuda_solver_energy(insem_cuda_solver* h, double* out, int32_t capacity, int32_t* n_out);
+/* Wavefield snapshots (Solver::record_snapshot, cpp/src/solver/solver.cpp:813-839;
+ * TimeConfig::snapshot_every / snapshot_quantities).  Set before the first
+ * step: every `every` steps, and at step 0, advance() records each of the
+ * `quantities` (insem_cuda_quantity: displacement, velocity, acceleration,
+ * pressure) of every medium that has it -- per quantity, media in domain
+ * order -- gathered to element points ([component][element][ngll^2], hanging
+ * points interpolated, azimuthal order 1 elastic as (U_r, U_theta, U_z)).
+ * every = 0 turns snapshots off.  Solves with snapshots step on their own
+ * (not streamed, not in a batch). */
+int insem_cuda_solver_set_snapshots(insem_cuda_solver* h, int32_t every, int32_t n_quantities,
+                                    const int32_t* quantities);
+int32_t insem_cuda_solver_n_snapshots(const insem_cuda_solver* h);        /* snapshots taken so far */
+int32_t insem_cuda_solver_n_snapshot_fields(const insem_cuda_solver* h);  /* recorded (medium, quantity) pairs */
+/* Medium, quantity, components and element points (elements x ngll^2) of a recorded field. */
+int insem_cuda_solver_snapshot_field(const insem_cuda_solver* h, int32_t field, int32_t* medium, int32_t* quantity,
+                                     int32_t* ncomp, int64_t* n_points);
+/* A field's snapshots: [n_snapshots][ncomp][n_points] floats. */
+int insem_cuda_solver_snapshot(const insem_cuda_solver* h, int32_t field, float* out);
+/* Times of the snapshots taken ([n_snapshots] doubles: step x dt). */
+int insem_cuda_solver_snapshot_times(const insem_cuda_solver* h, double* out);
 /* Current u, v, a of domain `domain` ([ncomp][n_global] host doubles; any may be NULL). */
 int insem_cuda_solver_state(insem_cuda_solver* h, int32_t domain, double* u, double* v, double* a);
 /* Device time of the last advance() call in milliseconds (CUDA events). */
@@ -335,12 +361,17 @@ int32_t insem_cuda_solver_tile_elements(const insem_cuda_solver* h, int32_t doma
  * counterpart in the reference: it adds an allocation-free form of the
  * internal_forces seam (solver.cpp:570-581).
  *   - Nothing is allocated or freed: the element-local force vectors go to a
- *     fixed 16 MiB device array inside the library (4,194,304 floats), which
- *     every GPU that loads the library holds until the process exits.  A
+ *     fixed 16 MiB device array inside the library (4,194,304 floats).  A
  *     domain needing more (ncomp x elements x ngll^2 floats) is rejected with
  *     INSEM_CUDA_ERR_UNSUPPORTED before anything is enqueued.
- *   - The first call on a device looks up the array's device address (once
- *     per device); make that first call before any stream capture.
+ *   - Under lazy module loading (the CUDA default) the driver reserves a
+ *     module's device memory when the module is first used.  Creating a
+ *     solver (insem_cuda_solver_create*) therefore loads the array and the
+ *     kernels this entry point runs, on the solver's device: the 16 MiB are
+ *     reserved then and held until the process exits, and calls here load
+ *     nothing.  Create the solver while device memory is still free.
+ *   - Each call looks up the array's device address on the current device
+ *     (a host-side lookup, nothing cached).
  *   - All calls share the array: calls whose work overlaps on the GPU (other
  *     streams, other threads, other handles) race on it.  Each call clears
  *     the part it uses before use. */

@@ -199,7 +199,8 @@ def run_timed_variant(variant: str, outdir: Path, only: list[str] | None) -> Non
         if variant == "double":
             ref = np.load(outdir / f"timed_{name}.npz")
             sim.set_time(n_steps=model.n_steps, duration=model.duration, dt=float(ref["meta.dt"]),
-                         safety=model.safety, record_every=model.record_every, energy_every=model.energy_every)
+                         safety=model.safety, record_every=model.record_every, energy_every=model.energy_every,
+                         snapshot_every=model.snapshot_every, snapshot_quantities=list(model.snapshot_quantities))
         solver = sim.solver
         n_full = int(solver.n_steps)
         n_run = n_full if n_run <= 0 else min(n_run, n_full)
@@ -224,6 +225,17 @@ def run_timed_variant(variant: str, outdir: Path, only: list[str] | None) -> Non
             for q in rec.quantities:
                 out[f"run.trace.{rec.name}.{q}"] = np.asarray(solver.trace(rec.name, q))
         out["run.energy"] = np.asarray(solver.energy).reshape(-1, 3)
+        if variant == "float" and model.snapshot_every > 0:
+            out["snap.times"] = np.asarray(solver.snapshot_times)
+            for medium in ("acoustic", "elastic"):
+                for q in model.snapshot_quantities:
+                    try:
+                        a = np.ascontiguousarray(np.asarray(solver.snapshot(medium, q)))
+                    except Exception:  # the medium does not have that quantity
+                        continue
+                    out[f"hash.snap.{medium}.{q}"] = np.asarray(digest(a))
+                    out[f"shape.snap.{medium}.{q}"] = np.asarray(a.shape, np.int64)
+                    out[f"norm.snap.{medium}.{q}"] = np.float64(np.linalg.norm(a.astype(np.float64)))
         if variant == "float":
             for di in range(len(rd.problem(solver)["domains"])):
                 f = rd.fields(solver, di)

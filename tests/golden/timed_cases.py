@@ -66,7 +66,8 @@ def ref_simulation(model, recipe):
         else:
             sim.add_receiver(r.name, r.x, r.z, list(r.quantities))
     sim.set_time(n_steps=model.n_steps, duration=model.duration, dt=model.dt, safety=model.safety,
-                 record_every=model.record_every, energy_every=model.energy_every)
+                 record_every=model.record_every, energy_every=model.energy_every,
+                 snapshot_every=model.snapshot_every, snapshot_quantities=list(model.snapshot_quantities))
     return sim
 
 

@@ -108,5 +108,36 @@ def stfs():
     return model, 0, ("rectangle", args, kw)
 
 
-TIMED = {"c2": c2, "c3s": c3s, "stfg": stfg, "stfs": stfs}
+def snapbh1():
+    """A short cased borehole at azimuthal order 1 (hanging faces, fluid-solid
+    coupling, the axis) recording wavefield snapshots of every quantity."""
+    b = K.borehole((-0.4, 0.64), [("mud", 0.1), ("casing", 0.11), ("cement", 0.14)], formation_radius=1.4, dz=0.08)
+    recipe = ("borehole", ((-0.4, 0.64), [("mud", 0.1), ("casing", 0.11), ("cement", 0.14)]),
+              dict(formation_radius=1.4, dz=0.08))
+    mats = {b.regions["mud"]: K.MUD, b.regions["casing"]: K.STEEL, b.regions["cement"]: K.CEMENT,
+            b.regions["formation"]: K.FAST}
+    model = K.Model(b.mesh, order=4, f_max=7500.0, azimuthal_order=1, materials=mats,
+                    boundaries={b.boundaries[n]: "absorbing" for n in ("bottom", "outer", "top")},
+                    sources=[K.Source("dipole", 0.0, 0.0, (1.0, 0.0, 0.0), K.ricker(3000.0))],
+                    receivers=[K.Receiver("p1", 0.05, 0.2, ["pressure"])], n_steps=240,
+                    snapshot_every=60, snapshot_quantities=("velocity", "pressure", "displacement", "acceleration"))
+    return model, 0, recipe
+
+
+def snaplay():
+    """Water over two curved elastic layers (Quad9 cells) recording velocity
+    and pressure snapshots, with a refined region (hanging faces)."""
+    interfaces = [-12.0, lambda x: -5.0 + 0.8 * np.sin(2 * np.pi * x / 9.0), 0.0, 4.0]
+    args, kw = ((0.0, 16.0), interfaces, [3, 2, 2], [1, 2, 0]), dict(nx=8, quadratic=True)
+    model = K.Model(
+        K.layered(*args, **kw), order=4, regions=[(4.0, 9.0, -8.0, -2.0, 1)],
+        materials={0: K.Material.acoustic(1500.0, 1000.0), 1: K.Material.elastic(3200.0, 1800.0, 2300.0),
+                   2: K.Material.elastic(2600.0, 1300.0, 2100.0)},
+        boundaries={K.BOTTOM: "absorbing", K.RIGHT: "absorbing", K.LEFT: "absorbing", K.TOP: "free"},
+        sources=[K.Source("force", 6.0, -3.0, (0.3, 1.0, 0.0), K.ricker(150.0))],
+        receivers=[K.Receiver("w0", 8.0, 2.0, ["pressure"])], n_steps=300, snapshot_every=75)
+    return model, 0, ("layered", args, kw)
+
+
+TIMED = {"c2": c2, "c3s": c3s, "stfg": stfg, "stfs": stfs, "snapbh1": snapbh1, "snaplay": snaplay}
 TIMED.update({f"c4m{k}": (lambda k=k: c4(k)) for k in C4_MODELS})

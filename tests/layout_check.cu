@@ -67,13 +67,13 @@ int main() {
             ++cases;
             const std::string id = "ng " + std::to_string(ng) + " kind " + std::to_string(kind) + " elastic " +
                                    std::to_string(elastic) + " m " + std::to_string(m) + " te " + std::to_string(te);
-            const uint32_t offs[] = {L.bar, L.metric, L.coef0, L.coef1, L.wr, L.hoop, L.r, L.desc,
-                                     L.u,   L.v,      L.im,    L.tf,    L.su, L.sfx,  L.ax, L.total};
+            const uint32_t offs[] = {L.bar, L.metric, L.wr, L.hoop, L.r,  L.u,  L.v,
+                                     L.im,  L.tf,     L.su, L.sfx,  L.ax, L.total};
             for (uint32_t o : offs)
               if (o % 16u) return fail(id + ": offset " + std::to_string(o) + " not 16-byte aligned");
             const uint32_t rows = static_cast<uint32_t>(rows_elem_stride(ng, nc));
             const uint32_t su_floats = rows > static_cast<uint32_t>(nc * npe) ? rows : static_cast<uint32_t>(nc * npe);
-            const uint32_t elem_end = TileLayout::up16(L.desc + 4u * te * L.cs);
+            const uint32_t elem_end = L.u;  // the element data runs up to the u region
             const Region bar{"barriers", L.bar, L.bar + 16};
             const Region elem{"element data", L.metric, elem_end};
             const Region u{"u", L.u, L.u + 4u * nc * tp_cap};

@@ -47,15 +47,17 @@ def test_served_results_equal_solo_runs(pkg):
 
 
 def test_small_budget_serialises_admission(pkg):
-    """With an HBM budget below two requests, each admission waits for the previous completion."""
+    """With an HBM budget that holds the largest request but no two requests,
+    each admission waits for the previous completion."""
     from insem_b200 import serving as S
 
     stream = _small_stream()[:5]
-    recs = S.Server(hbm_budget=1, chunk_steps=16).run(stream, keep_traces=False)
+    budget = max(S._stage_host(r)[3] for r in stream)
+    recs = S.Server(hbm_budget=budget, chunk_steps=16).run(stream, keep_traces=False)
     order = sorted(recs.values(), key=lambda r: r.admitted)
     for a, b in zip(order, order[1:]):
         assert b.admitted >= a.completed
-    assert all(np.isfinite(r.completed) for r in recs.values())
+    assert all(np.isfinite(r.completed) and r.status == "done" for r in recs.values())
 
 
 def test_plain_server_runs_the_same_stream(pkg):
@@ -99,3 +101,45 @@ def test_timed_constructor_matches_two_step_route(pkg):
     with pytest.raises(N.InsemError) as e:
         K.build_solver_from_arrays(model, arrays)
     assert e.value.code == N.ERR_INVALID and "stability limit" in str(e.value)
+
+
+def _poison(solver):
+    """Initial state with one NaN (host-side fault injection through set_state)."""
+    medium = solver.media[0]
+    u, v, _ = solver.state(medium)
+    u = np.array(u, copy=True)
+    u[0, u.shape[1] // 2] = np.nan
+    solver.set_state(medium, u, v)
+
+
+def test_nonfinite_request_is_evicted_and_the_mix_is_unaffected(pkg):
+    """One request of a running mix goes non-finite (a NaN in its initial
+    state): it is marked failed and evicted, and every other request's traces
+    still equal its solo run, bit for bit."""
+    from insem_b200 import serving as S
+
+    stream = _small_stream()[:6]
+    target = stream[2]
+    target.init = _poison
+    recs = S.Server(chunk_steps=7).run(stream)
+    bad = recs[target.rid]
+    assert bad.status == "failed" and "NaN" in bad.error, (bad.status, bad.error)
+    summ = S.summarize(recs)
+    assert summ["completed"] == len(stream) - 1 and summ["failed"] == 1
+    for r in stream:
+        if r is target:
+            continue
+        rec = recs[r.rid]
+        assert rec.status == "done"
+        assert np.array_equal(rec.traces, _solo_traces(r)), (r.rid, r.kind)
+
+
+def test_plain_server_isolates_a_nonfinite_request(pkg):
+    from insem_b200 import serving as S
+
+    stream = _small_stream()[:3]
+    stream[1].init = _poison
+    recs = S.serve_plain(stream, keep_traces=True)
+    assert recs[stream[1].rid].status == "failed"
+    for r in (stream[0], stream[2]):
+        assert recs[r.rid].status == "done" and np.array_equal(recs[r.rid].traces, _solo_traces(r))

@@ -6,8 +6,8 @@ boreholes over 12,000 steps, the Gaussian and sampled source time functions).
 The models are built by the native case builder, whose arrays the CPU test
 ``test_timed_builder.py`` proves equal to the reference's setup.  Two runs:
 
-* at the reference float build's dt: receiver traces and sample times bit for
-  bit (SHA-256 of all samples; the fixture keeps every k-th row besides, to
+* at the reference float build's dt: receiver traces, sample times and (where
+  the model records them) wavefield snapshots bit for bit (SHA-256 of all samples; the fixture keeps every k-th row besides, to
   report the size of a difference), the final u, v, a of every domain bit for
   bit (SHA-256 of the float32 fields in the reference's point numbering),
   energy to 1e-9 relative;
@@ -47,6 +47,21 @@ def _problem(pkg, case):
     return z, model, arrays
 
 
+def _check_snapshots(s, z, case):
+    """Device snapshots against the reference's (Solver::record_snapshot): same
+    times, and every recorded (medium, quantity) field bit for bit."""
+    assert np.array_equal(s.snapshot_times, z["snap.times"]), case
+    keys = [k[len("hash.snap."):] for k in z.files if k.startswith("hash.snap.")]
+    assert keys
+    for key in keys:
+        medium, quantity = key.split(".")
+        got = np.ascontiguousarray(s.snapshot(medium, quantity))
+        assert list(got.shape) == list(z[f"shape.snap.{key}"]), (case, key)
+        norm = np.linalg.norm(got.astype(np.float64))
+        assert _digest(got) == str(z[f"hash.snap.{key}"]), \
+            f"{case} {key}: norm {norm:.9e} vs {float(z[f'norm.snap.{key}']):.9e}"
+
+
 @pytest.mark.parametrize("case", TIMED)
 def test_reference_dt_run_bitwise(pkg, case):
     from insem_b200 import cases as K
@@ -57,9 +72,13 @@ def test_reference_dt_run_bitwise(pkg, case):
     prob.dt = float(z["meta.dt"])
     prob.n_steps = n_run
     with pkg.Solver(prob) as s:
+        if model.snapshot_every > 0:
+            s.set_snapshots(model.snapshot_every, model.snapshot_quantities)
         s.advance(n_run // 3)
         s.run()
         assert s.step == n_run
+        if model.snapshot_every > 0:
+            _check_snapshots(s, z, case)
         stride = int(z["meta.trace_stride"])
         assert _digest(s.times) == str(z["hash.run.times"])
         for name, q in prob.trace_list():

@@ -58,3 +58,59 @@ def test_shipped_tile_table_registers(pkg):
     finally:
         for k, te in before.items():
             autotune.register(k, te)
+
+
+def test_pipeline_isolates_failing_and_oversize_requests(pkg, monkeypatch):
+    """Host-side failures stay with their request: a request whose setup fails
+    (its source lies outside the model) is marked failed with the setup error,
+    a request larger than the whole HBM budget is rejected instead of being
+    admitted into an empty GPU, and every other request goes through.  The
+    device stage is replaced by a stand-in, so this runs without a GPU."""
+    import time
+
+    from insem_b200 import serving as S
+
+    stream = S.request_stream(rate=300.0, window=1.0, time_scale=0.004, max_requests=6)
+    for r in stream:
+        if r.kind.startswith("cartesian"):
+            r.spec["elements"] = 2000.0
+    bad, big = stream[1].rid, stream[3].rid
+    real_model, real_host = S.request_model, S._stage_host
+
+    def model_with_a_stray_source(req):
+        m = real_model(req)
+        if req.rid == bad:
+            m.sources[0].x, m.sources[0].z = 1.0e6, 1.0e6
+        return m
+
+    def host_stage(req):
+        model, arrays, ne, need = real_host(req)
+        return model, arrays, ne, need * 1000 if req.rid == big else need
+
+    class Done:
+        n_steps = 1
+
+        @staticmethod
+        def n_global_total():
+            return 1
+
+    monkeypatch.setattr(S, "request_model", model_with_a_stray_source)
+    monkeypatch.setattr(S, "_stage_host", host_stage)
+    monkeypatch.setattr(S, "_stage_device", lambda *a, **k: (Done(), object()))
+    needs = [real_host(r)[3] for r in stream if r.rid not in (bad, big)]
+    recs = {r.rid: S.Record(r.rid, r.kind, r.arrival) for r in stream}
+    pipe = S._Pipeline(stream, recs, 0, 10 * max(needs), 2, True, False)
+    served = []
+    t_end = time.time() + 60.0
+    try:
+        while pipe.pending() and time.time() < t_end:
+            for rid, _, _, need in pipe.poll(0):
+                served.append(rid)
+                pipe.release(need)
+            pipe.idle_wait()
+    finally:
+        pipe.close()
+    assert recs[bad].status == "failed" and "not inside" in recs[bad].error
+    assert recs[big].status == "rejected" and "budget" in recs[big].error
+    assert sorted(served) == sorted(r.rid for r in stream if r.rid not in (bad, big))
+    assert pipe.used == 0

@@ -18,7 +18,7 @@ import pytest
 
 from conftest import GOLDEN
 
-TIMED = ["c2", "c3s", "stfg", "stfs", "c4m0", "c4m1", "c4m12", "c4m17", "c4m72", "c4m80"]
+TIMED = ["c2", "c3s", "stfg", "stfs", "snapbh1", "snaplay", "c4m0", "c4m1", "c4m12", "c4m17", "c4m72", "c4m80"]
 SKIP = ("problem.dt", "problem.stable_dt", "problem.n_steps", "problem.real_bytes")
 
 
@@ -65,3 +65,31 @@ def test_builder_matches_reference_on_benchmarked_models(pkg, case):
         checked += 1
     assert not mismatched, f"arrays differing from the reference's setup: {mismatched[:8]}"
     assert checked > 20
+
+
+# Error of the float build (and so of the CUDA path, which equals it bit for
+# bit) against the FP64 build (INSEM_REAL=double) on the benchmarked models,
+# as stated in the design notes: worst receiver-trace relative L2 error, and
+# the float build's total energy against the FP64 build's, relative to the
+# largest FP64 energy.  Both builds run the same dt and steps.
+FP64_BOUNDS = {  # case: (trace rel-L2, energy)
+    "c2": (2e-5, 3e-6), "c3s": (6e-5, 3e-6), "c4m0": (2e-5, 6e-6), "c4m1": (8e-5, 1e-6),
+    "c4m12": (2e-5, 1e-6), "c4m17": (3e-5, 1e-6), "c4m72": (6e-5, 3e-6), "c4m80": (3e-5, 1e-6),
+    "stfg": (4e-4, 1e-6), "stfs": (1e-6, 1e-6), "snapbh1": (3e-6, None), "snaplay": (3e-6, None),
+}
+
+
+@pytest.mark.parametrize("case", TIMED)
+def test_float_build_error_against_fp64(case):
+    import golden_io as G
+
+    z, d = timed_fixture(case), np.load(GOLDEN / f"timed_{case}_f64.npz")
+    assert float(z["meta.dt"]) == float(d["meta.dt"]) and int(z["meta.n_steps_run"]) == int(d["meta.n_steps_run"])
+    worst = max(G.rel_l2(z[k], d[k]) for k in z.files if k.startswith("run.trace."))
+    trace_bound, energy_bound = FP64_BOUNDS[case]
+    assert worst <= trace_bound, worst
+    if energy_bound is not None:  # the model records the energy monitor
+        e32, e64 = z["run.energy"], d["run.energy"]
+        tot32, tot64 = e32[:, 1] + e32[:, 2], e64[:, 1] + e64[:, 2]
+        energy = float(np.abs(tot32 - tot64).max() / np.abs(tot64).max())
+        assert energy <= energy_bound, energy
