@@ -70,7 +70,7 @@ void DeviceDomainData::upload(const insem_cuda_domain& d, const insem_cuda_basis
   zero_idx.upload(z);
 }
 
-void DeviceDomainData::alloc_fields() {
+void DeviceDomainData::alloc_fields(cudaStream_t s) {
   if (fields_ready) return;
   const std::size_t nf = static_cast<std::size_t>(ncomp) * ng;
   u.resize(nf);
@@ -78,11 +78,13 @@ void DeviceDomainData::alloc_fields() {
   a.resize(nf);
   f.resize(nf);
   f_local.resize(static_cast<std::size_t>(ncomp) * n_elements * npe);
-  u.zero();
-  v.zero();
-  a.zero();
-  f.zero();
-  f_local.zero();
+  // zeroed in the order of the stream that uses them next (a memset on the
+  // default stream is not ordered with the solver's non-blocking streams)
+  u.zero(s);
+  v.zero(s);
+  a.zero(s);
+  f.zero(s);
+  f_local.zero(s);
   fields_ready = true;
 }
 
@@ -352,7 +354,7 @@ AllFields Solver::fields_view() {
 }
 
 void Solver::internal_forces(DeviceDomainData& d, const float* u_global, float* f_global) {
-  d.alloc_fields();
+  d.alloc_fields(stream);
   for (const DeviceBlock& b : d.blocks) {
     ElementLaunch a;
     a.basis = basis.view();
@@ -468,7 +470,7 @@ void Solver::replay(int n, const std::function<void()>& body) {
 // with x ~ U(-1, 1) from mt19937(12345), Rayleigh quotients in double.
 double Solver::stable_dt() {
   DeviceGuard dg(device);
-  for (auto& d : domains) d.alloc_fields();
+  for (auto& d : domains) d.alloc_fields(stream);
   std::mt19937 rng(12345);
   std::uniform_real_distribution<double> dist(-1.0, 1.0);
   DeviceBuffer<double> pw(kPwCount);

@@ -28,7 +28,7 @@ struct DeviceDomainData {
   DeviceBuffer<int64_t> zero_idx;
   DeviceBuffer<float> u, v, a, f, f_local;  // two-pass path only (alloc_fields)
   bool fields_ready = false;
-  void alloc_fields();
+  void alloc_fields(cudaStream_t s = nullptr);
   void free_fields();
 
   void upload(const insem_cuda_domain& d, const insem_cuda_basis& basis);
