@@ -177,21 +177,20 @@ __device__ __forceinline__ void load_metric(const float* metric, int b, int k, f
 // block data: f_xi / f_eta per component, the direct (hoop) terms, and for
 // axis points of axial elements the axis terms g xi_r, g eta_r (stored at
 // row j of gx*/gy*).  The body of each reference kernel's first loop.
-// ECOEF: blk.coef0 / coef1 hold one value per element (the material is one
-// per element, so every point of it carries the same coefficients) instead
-// of one per point.
+// ECOEF: the element's coefficients come in as ec0 / ec1 (the material is
+// one per element, so every point of it carries the same coefficients; the
+// caller reads them once) instead of from blk.coef0 / coef1 per point.
 template <int NG, int KIND, bool ELASTIC, int M, bool ECOEF = false>
 __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt, int i, int j, bool axial,
                                            const float* uxi, const float* ueta, const float* upt, float* fx,
                                            float* fy, float* direct, float* gx0, float* gy0, float* gx1,
-                                           float* gy1, float w2k) {
+                                           float* gy1, float w2k, float ec0 = 0.0f, float ec1 = 0.0f) {
   constexpr int NPE = NG * NG;
   constexpr int CS = point_stride<NPE>();
   if constexpr (KIND != INSEM_AXISYM) {
     float xi_x, xi_z, eta_x, eta_z, jac;
     load_metric<KIND, NPE>(blk.metric, bb, kpt, xi_x, xi_z, eta_x, eta_z, jac);
     const size_t p = static_cast<size_t>(bb) * CS + kpt;
-    const size_t pc = ECOEF ? static_cast<size_t>(bb) : p;
     if constexpr (ELASTIC) {
       // elastic_kernel (kernels.cpp:64-120)
       float ux_x, ux_z, uz_x, uz_z;
@@ -205,7 +204,7 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
         phys_grad(uxi[1], ueta[1], xi_x, xi_z, eta_x, eta_z, uz_x, uz_z);
       }
       float sxx, szz, sxz;
-      el_stress(blk.coef0[pc], blk.coef1[pc], ux_x, ux_z, uz_x, uz_z, sxx, szz, sxz);
+      el_stress((ECOEF ? ec0 : blk.coef0[p]), (ECOEF ? ec1 : blk.coef1[p]), ux_x, ux_z, uz_x, uz_z, sxx, szz, sxz);
       const float wj = fmul(w2k, jac);
       if constexpr (KIND == INSEM_RECT) {
         fx[0] = fmul(fmul(wj, sxx), xi_x);
@@ -218,7 +217,7 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
       }
     } else {
       // acoustic_kernel (kernels.cpp:122-158)
-      const float c = fmul(fmul(w2k, jac), blk.coef0[pc]);
+      const float c = fmul(fmul(w2k, jac), (ECOEF ? ec0 : blk.coef0[p]));
       if constexpr (KIND == INSEM_RECT) {
         fx[0] = fmul(fmul(fmul(c, uxi[0]), xi_x), xi_x);
         fy[0] = fmul(fmul(fmul(c, ueta[0]), eta_z), eta_z);
@@ -230,7 +229,6 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
     }
   } else {
     const size_t p = static_cast<size_t>(bb) * CS + kpt;
-    const size_t pc = ECOEF ? static_cast<size_t>(bb) : p;
     const float* mt = blk.metric + static_cast<size_t>(bb) * 4 * CS + kpt;
     const float xi_r = mt[0], xi_z = mt[CS], eta_r = mt[2 * CS], eta_z = mt[3 * CS];
     const bool axis_pt = axial && i == 0;
@@ -241,7 +239,7 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
       phys_grad(uxi[1], ueta[1], xi_r, xi_z, eta_r, eta_z, uz_r, uz_z);
       const float r = blk.r[p];
       const float e_tt = r == 0.0f ? ur_r : __fdiv_rn(upt[0], r);
-      const float lambda = blk.coef0[pc], mu = blk.coef1[pc];
+      const float lambda = (ECOEF ? ec0 : blk.coef0[p]), mu = (ECOEF ? ec1 : blk.coef1[p]);
       const float tr = fadd(fadd(ur_r, uz_z), e_tt);
       const float two_mu = fmul(2.0f, mu);
       const float ltr = fmul(lambda, tr);
@@ -264,7 +262,7 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
       // acoustic_axisym_kernel (kernels.cpp:265-294)
       float p_r, p_z;
       phys_grad(uxi[0], ueta[0], xi_r, xi_z, eta_r, eta_z, p_r, p_z);
-      ref_flux(fmul(blk.wr[p], blk.coef0[pc]), p_r, p_z, xi_r, xi_z, eta_r, eta_z, fx[0], fy[0]);
+      ref_flux(fmul(blk.wr[p], (ECOEF ? ec0 : blk.coef0[p])), p_r, p_z, xi_r, xi_z, eta_r, eta_z, fx[0], fy[0]);
     } else if constexpr (ELASTIC && M == 1) {
       // elastic_axisym1_kernel (kernels.cpp:305-385)
       const float s2 = 1.41421356237309504880f;
@@ -280,7 +278,7 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
       const float ur_r = fmul(fadd(up_r, um_r), is2), ur_z = fmul(fadd(up_z, um_z), is2);
       const float ut_r = fmul(fsub(up_r, um_r), is2), ut_z = fmul(fsub(up_z, um_z), is2);
       const float e_tt = fmul(s2, up_over_r);
-      const float lambda = blk.coef0[pc], mu = blk.coef1[pc];
+      const float lambda = (ECOEF ? ec0 : blk.coef0[p]), mu = (ECOEF ? ec1 : blk.coef1[p]);
       const float tr = fadd(fadd(ur_r, uz_z), e_tt);
       const float two_mu = fmul(2.0f, mu);
       const float ltr = fmul(lambda, tr);
@@ -312,7 +310,7 @@ __device__ __forceinline__ void point_flux(const BlockDev& blk, int bb, int kpt,
       // acoustic_axisym1_kernel (kernels.cpp:389-431)
       float p_r, p_z;
       phys_grad(uxi[0], ueta[0], xi_r, xi_z, eta_r, eta_z, p_r, p_z);
-      const float inv_rho = blk.coef0[pc];
+      const float inv_rho = (ECOEF ? ec0 : blk.coef0[p]);
       const float wri = fmul(blk.wr[p], inv_rho);
       ref_flux(wri, p_r, p_z, xi_r, xi_z, eta_r, eta_z, fx[0], fy[0]);
       if (axis_pt) {

@@ -251,7 +251,10 @@ struct TileLayout {
     // su doubles as the halo staging area: [te][nc][npe]
     o = up16(o + 4u * te * (rows > static_cast<uint32_t>(nc * npe) ? rows : static_cast<uint32_t>(nc * npe)));
     const uint32_t sfx_b = up16(4u * te * rows);
-    if (sfx_b <= elem) {
+    // three-component classes write their f_xi rows as the fluxes are formed
+    // (fewer registers held across the barrier), so their rows cannot sit in
+    // the element data the fluxes still read
+    if (sfx_b <= elem && nc != 3) {
       L.sfx = L.metric;
     } else {
       L.sfx = o;
@@ -392,10 +395,13 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   const int i = tid - el * NG;
   const bool active = el < th.ne;
   uint32_t dsc[NG];
+  float ec0 = 0.0f, ec1 = 0.0f;  // the element's material coefficients
   if (active) {
     const uint32_t* gdesc = td.sdesc + static_cast<size_t>(th.be0 + el) * CS + i;
 #pragma unroll
     for (int j = 0; j < NG; ++j) dsc[j] = gdesc[j * NG];
+    ec0 = blk.coef0[th.be0 + el];
+    if constexpr (EL) ec1 = blk.coef1[th.be0 + el];
   }
   // halo tile points, gathered while the bulk copies are in flight
   for (int t = tid; t < th.ntp - th.nc; t += nthreads) {
@@ -411,12 +417,11 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     return false;
   }
 
-  // element data now in shared memory, indexed by the tile-local element;
-  // the coefficients (one pair per element) stay in global memory
+  // element data now in shared memory, indexed by the tile-local element
   BlockDev lb = blk;
   lb.metric = s_metric;
-  lb.coef0 = blk.coef0 + th.be0;
-  lb.coef1 = EL ? blk.coef1 + th.be0 : nullptr;
+  lb.coef0 = nullptr;  // one pair per element: ec0 / ec1
+  lb.coef1 = nullptr;
   lb.wr = s_wr;
   lb.hoop = s_hoop;
   lb.r = s_r;
@@ -495,7 +500,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
         float uxi[NC] = {av.x, av.y}, ueta[NC] = {bv.x, bv.y}, upt[NC] = {ucol[0][j], ucol[1][j]};
         float fxp[NC], fy[NC], dr[2] = {0.0f, 0.0f};
         point_flux<NG, KIND, EL, M, true>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
-                                    ax + 3 * AXS, w2c[j]);
+                                    ax + 3 * AXS, w2c[j], ec0, ec1);
         fx[0][j] = fxp[0];
         fx[1][j] = fxp[1];
         fe[0][j] = fy[0];
@@ -528,10 +533,11 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 #pragma unroll
         for (int c = 0; c < NC; ++c) upt[c] = ucol[c][j];
         point_flux<NG, KIND, EL, M, true>(lb, el, k, i, j, axial, uxi, ueta, upt, fxp, fy, dr, ax, ax + AXS, ax + 2 * AXS,
-                                    ax + 3 * AXS, w2c[j]);
+                                    ax + 3 * AXS, w2c[j], ec0, ec1);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          fx[c][j] = fxp[c];
+          if constexpr (NC == 3) frow[ridx(c, j, i)] = fxp[c];  // own region: store now
+          else fx[c][j] = fxp[c];
           fe[c][j] = fy[c];
         }
         dir[0][j] = dr[0];
@@ -540,7 +546,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     }
   }
   __syncthreads();  // the element data is dead: the f_xi rows may overwrite it
-  if (active) {
+  if (active && NC != 3) {
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
       if constexpr (PAIR) {
