@@ -536,7 +536,7 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
     ap.add_argument("--serve-rate", type=float, default=50.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-window", type=float, default=3.0, help="serving: seconds of arrivals at --serve-rate")
-    ap.add_argument("--serve-rates", default="2,4",
+    ap.add_argument("--serve-rates", default="1,2,3",
                     help="serving: arrival rates (per s) one GPU sustains, measured besides --serve-rate")
     ap.add_argument("--serve-window-sustained", type=float, default=8.0,
                     help="serving: seconds of arrivals at each of --serve-rates")
