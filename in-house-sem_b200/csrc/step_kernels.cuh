@@ -203,11 +203,32 @@ struct AllFields {
   DomainFields d[2];
 };
 
-__device__ __forceinline__ double interp(const ReceiversDev& r, int32_t rec, const float* field, int32_t ng, int c) {
+// sum over q = beg .. end-1 of (double)coef[q] * (double)field[pts[q]], added
+// in ascending q (the reference's order); the loads of four terms are issued
+// before their four additions, so their latencies overlap.
+__device__ __forceinline__ double ordered_dot(const float* __restrict__ coef, const int32_t* __restrict__ pts,
+                                              int32_t beg, int32_t end, const float* __restrict__ field) {
   double s = 0.0;
-  for (int32_t q = r.offsets[rec]; q < r.offsets[rec + 1]; ++q)
-    s = dadd(s, dmul(static_cast<double>(r.value[q]), static_cast<double>(field[static_cast<size_t>(c) * ng + r.points[q]])));
+  int32_t q = beg;
+  for (; q + 4 <= end; q += 4) {
+    int32_t p[4];
+    float c[4], f[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) p[k] = pts[q + k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      c[k] = coef[q + k];
+      f[k] = field[p[k]];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) s = dadd(s, dmul(static_cast<double>(c[k]), static_cast<double>(f[k])));
+  }
+  for (; q < end; ++q) s = dadd(s, dmul(static_cast<double>(coef[q]), static_cast<double>(field[pts[q]])));
   return s;
+}
+
+__device__ __forceinline__ double interp(const ReceiversDev& r, int32_t rec, const float* field, int32_t ng, int c) {
+  return ordered_dot(r.value, r.points, r.offsets[rec], r.offsets[rec + 1], field + static_cast<size_t>(c) * ng);
 }
 
 // Particle velocity of acoustic receivers: trapezoid of -grad(p)/rho.  With
@@ -218,12 +239,9 @@ __device__ __forceinline__ void particle_velocity_body(const ReceiversDev& r, co
   if (t >= n_acoustic) return;
   const int32_t rec = acoustic_recv[t];
   const DomainFields& d = fl.d[r.domain[rec]];
-  double gx = 0.0, gz = 0.0;
-  for (int32_t q = r.offsets[rec]; q < r.offsets[rec + 1]; ++q) {
-    const double u = static_cast<double>(d.u[r.points[q]]);
-    gx = dadd(gx, dmul(static_cast<double>(r.d_dx[q]), u));
-    gz = dadd(gz, dmul(static_cast<double>(r.d_dz[q]), u));
-  }
+  // two independent sums, each in ascending point order
+  const double gx = ordered_dot(r.d_dx, r.points, r.offsets[rec], r.offsets[rec + 1], d.u);
+  const double gz = ordered_dot(r.d_dz, r.points, r.offsets[rec], r.offsets[rec + 1], d.u);
   const double ax = __ddiv_rn(-gx, r.rho[rec]), az = __ddiv_rn(-gz, r.rho[rec]);
   double* pv = r.pv + static_cast<size_t>(rec) * 4;
   if (!init) {
