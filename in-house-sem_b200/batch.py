@@ -2,7 +2,8 @@
 
 Every batched step is one CUDA graph with a fixed number of launches,
 whatever the number of problems:
-- one tile kernel per tile class, whose CTAs pull tiles from a device queue;
+- one tile kernel per tile class, one CTA per tile; the classes spread over
+  ``tile_streams`` streams (default 2) and run side by side;
 - then the point-wise kernels of all problems run.
 
 Each problem keeps its own time step and step count. A problem's results in
@@ -43,8 +44,8 @@ class BatchMember(Solver):
 
 
 class Batch:
-    def __init__(self, device: int = 0, use_graphs: bool = True, check_finite: bool = True):
-        opts = N.Options(device, int(use_graphs), 0, 0, int(check_finite))
+    def __init__(self, device: int = 0, use_graphs: bool = True, check_finite: bool = True, tile_streams: int = 0):
+        opts = N.Options(device, int(use_graphs), 0, 0, int(check_finite), int(tile_streams))
         h = C.c_void_p()
         N.check(N.lib().insem_cuda_batch_create(C.byref(opts), C.byref(h)))
         self._h = h

@@ -82,7 +82,6 @@ void Solver::batch_collect(BatchTables& T) {
       sg.sc = sc;
       sg.st = st;
       sg.epartial = epart.get() + 2 * static_cast<std::size_t>(ep_tile[di]);
-      sg.tile0 = bt.tile0;
       const int m = bt.kind == INSEM_AXISYM ? bt.m : 0;
       const int key = ((ngll * 4 + bt.kind) * 2 + (el ? 1 : 0)) * 2 + m;
       TileClass& c = T.tiles[key];
@@ -96,7 +95,14 @@ void Solver::batch_collect(BatchTables& T) {
       c.nc_cap = std::max(c.nc_cap, t.nc_cap);
       const int32_t seg = static_cast<int32_t>(c.segs.size());
       c.segs.push_back(sg);
-      for (int k = 0; k < bt.ntiles; ++k) c.items.push_back(int2{seg, k});
+      for (int k = 0; k < bt.ntiles; ++k) {
+        TileItem it{};
+        it.th = t.host_tiles[bt.tile0 + k];
+        it.st = st;
+        it.seg = seg;
+        it.tile = bt.tile0 + k;
+        c.items.push_back(it);
+      }
     }
   }
   CouplingDev cp{tcpl_fluid.get(), tcpl_solid.get(), cpl_cx.get(), cpl_cz.get()};
@@ -204,9 +210,14 @@ Batch::Batch(const insem_cuda_options* opt) {
   CUDA_CHECK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   CUDA_CHECK(cudaEventCreate(&ev0));
   CUDA_CHECK(cudaEventCreate(&ev1));
-  CUDA_CHECK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+  INSEM_REQUIRE(opts.tile_streams >= 0 && opts.tile_streams <= kMaxLanes, INSEM_CUDA_ERR_INVALID,
+                "tile_streams must be 0..8");
+  n_lanes = opts.tile_streams > 0 ? opts.tile_streams : 2;
   CUDA_CHECK(cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming));
-  CUDA_CHECK(cudaEventCreateWithFlags(&join_ev, cudaEventDisableTiming));
+  for (int k = 0; k + 1 < n_lanes; ++k) {
+    CUDA_CHECK(cudaStreamCreateWithFlags(&lanes[k], cudaStreamNonBlocking));
+    CUDA_CHECK(cudaEventCreateWithFlags(&join_ev[k], cudaEventDisableTiming));
+  }
   CUDA_CHECK(cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, opts.device));
   CUDA_CHECK(cudaMallocHost(&herr, sizeof(int32_t)));
   derr.resize(1);
@@ -216,15 +227,18 @@ Batch::~Batch() {
   DeviceGuard dg(opts.device);
   // members' buffers are released below: both streams must be done with them
   if (stream) cudaStreamSynchronize(stream);
-  if (side) cudaStreamSynchronize(side);
+  for (cudaStream_t l : lanes)
+    if (l) cudaStreamSynchronize(l);
   if (graph) cudaGraphExecDestroy(graph);
   members.clear();
   if (herr) cudaFreeHost(herr);
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (fork_ev) cudaEventDestroy(fork_ev);
-  if (join_ev) cudaEventDestroy(join_ev);
-  if (side) cudaStreamDestroy(side);
+  for (cudaEvent_t e : join_ev)
+    if (e) cudaEventDestroy(e);
+  for (cudaStream_t l : lanes)
+    if (l) cudaStreamDestroy(l);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -301,6 +315,7 @@ void Batch::rebuild() {
     s.batch_collect(T);
   }
   dclasses.clear();
+  std::vector<std::pair<double, std::size_t>> work;  // (elements x points per element x components, class)
   for (auto& kv : T.tiles) {
     TileClass& c = kv.second;
     DevClass d;
@@ -323,11 +338,22 @@ void Batch::rebuild() {
     const int per_sm = std::max(1, tile_batch(c.ngll, a, false));
     // one CTA per item (the call above also sets the kernel's shared memory size)
     (void)per_sm;
-    d.grid = std::max(1, d.n_items);
+    d.grid = d.n_items;  // CTA b reads item b: no launch without items
+    double w = 0.0;
+    for (const TileItem& it : c.items) w += static_cast<double>(it.th.ne);
+    work.emplace_back(w * c.ngll * c.ngll * c.ncomp, dclasses.size());
     dclasses.push_back(std::move(d));
   }
-  if (queues.size() != std::max<std::size_t>(dclasses.size(), 1)) queues.resize(std::max<std::size_t>(dclasses.size(), 1));
-  queues.zero(stream);
+  {
+    // lanes: classes by work, largest first, each to the least loaded lane
+    std::sort(work.begin(), work.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<double> load(n_lanes, 0.0);
+    for (const auto& w : work) {
+      const int l = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+      dclasses[w.second].lane = l;
+      load[l] += w.first;
+    }
+  }
   for (int c = 0; c < 3; ++c) {
     dhalo_segs[c].upload_async(T.halo_segs[c], stream);
     dhalo_items[c].upload_async(T.halo_items[c], stream);
@@ -381,41 +407,38 @@ void Batch::rebuild() {
 
 void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
   const int32_t nq = static_cast<int32_t>(dclasses.size());
-  const int32_t nb = std::max(n_states, nq);
-  batch_begin_kernel<<<ceil_div(std::max(nb, 1), 256), 256, 0, stream>>>(dstates.get(), n_states, queues.get(), nq);
+  batch_begin_kernel<<<ceil_div(std::max(n_states, 1), 256), 256, 0, stream>>>(dstates.get(), n_states);
   CUDA_LAUNCH_CHECK();
   if (n_cons_items > 0) {
     constrained_batch_kernel<<<n_cons_items, kConsChunk, 0, stream>>>(dcons_segs.get(), dcons_items.get());
     CUDA_LAUNCH_CHECK();
   }
   if (tiles_begin) CUDA_CHECK(cudaEventRecord(tiles_begin, stream));
-  bool any_el = false, any_ac = false;
-  for (const DevClass& d : dclasses) (d.elastic ? any_el : any_ac) = true;
-  const bool split = any_el && any_ac;
-  if (split) {
+  int used = 1;  // lanes in use: 0 .. used-1
+  for (const DevClass& d : dclasses) used = std::max(used, d.lane + 1);
+  if (used > 1) {
     CUDA_CHECK(cudaEventRecord(fork_ev, stream));
-    CUDA_CHECK(cudaStreamWaitEvent(side, fork_ev, 0));
+    for (int k = 1; k < used; ++k) CUDA_CHECK(cudaStreamWaitEvent(lanes[k - 1], fork_ev, 0));
   }
   for (int32_t q = 0; q < nq; ++q) {
     const DevClass& d = dclasses[q];
+    if (d.n_items == 0) continue;
     TileBatchLaunch a;
     a.kind = d.kind;
     a.m = d.m;
     a.elastic = d.elastic;
     a.segs = d.segs.get();
     a.items = d.items.get();
-    a.n_items = d.n_items;
-    a.queue = queues.get() + q;
     a.te = d.te;
     a.L = d.L;
     a.smem = d.L.total;
     a.grid = d.grid;
-    a.stream = split && !d.elastic ? side : stream;
+    a.stream = d.lane == 0 ? stream : lanes[d.lane - 1];
     tile_batch(d.ngll, a, true);
   }
-  if (split) {
-    CUDA_CHECK(cudaEventRecord(join_ev, side));
-    CUDA_CHECK(cudaStreamWaitEvent(stream, join_ev, 0));
+  for (int k = 1; k < used; ++k) {
+    CUDA_CHECK(cudaEventRecord(join_ev[k - 1], lanes[k - 1]));
+    CUDA_CHECK(cudaStreamWaitEvent(stream, join_ev[k - 1], 0));
   }
   if (tiles_end) CUDA_CHECK(cudaEventRecord(tiles_end, stream));
   // solid halos first: the fluid's coupling term reads the solid's new acceleration

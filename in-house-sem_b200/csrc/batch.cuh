@@ -6,8 +6,8 @@
 // the number of solves:
 //   begin (step counters, buffer parities, modes; tile queues reset)
 //   constrained-slot gathers of every solve
-//   one tile launch per tile class (ngll, kind, medium, order): each CTA
-//     pulls a (segment, tile) item from a device work queue
+//   one tile launch per tile class (ngll, kind, medium, order): one CTA
+//     per (segment, tile) item
 //   halo points of every solve (elastic classes, then acoustic: the fluid's
 //     coupling term reads the solid's new acceleration)
 //   receivers (particle velocity, then recording) and energy of every solve
@@ -41,7 +41,7 @@ struct TileClass {
   bool elastic = false;
   int tp_cap = 0, nc_cap = 0, te = 0;  // largest tile of the class
   std::vector<TileSeg> segs;
-  std::vector<int2> items;
+  std::vector<TileItem> items;
 };
 
 // Host-side segment tables of one batch composition.
@@ -107,8 +107,9 @@ class Batch {
     int ngll = 0, kind = 0, m = 0;
     bool elastic = false;
     DeviceBuffer<TileSeg> segs;
-    DeviceBuffer<int2> items;
+    DeviceBuffer<TileItem> items;
     int32_t n_items = 0;
+    int lane = 0;
     int te = 0;
     TileLayout L{};
     int grid = 0;
@@ -116,11 +117,17 @@ class Batch {
 
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  // acoustic tile classes run on `side`, beside the elastic ones (neither
-  // reads what the other writes), forked after the constrained gathers and
-  // joined before the halo kernels
-  cudaStream_t side = nullptr;
-  cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
+  // The tile classes of a step run side by side on `n_lanes` streams (lane 0
+  // is `stream`, lane k > 0 is lanes[k - 1]): no tile writes what another
+  // tile reads (complete points belong to one tile, halo contributions have
+  // their own places), so classes need no order among them.  The lanes fork
+  // after the constrained gathers and join before the halo kernels.  Classes
+  // go to lanes largest first, each to the lane with the least work.
+  static constexpr int kMaxLanes = 8;
+  int n_lanes = 1;
+  cudaStream_t lanes[kMaxLanes - 1] = {};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[kMaxLanes - 1] = {};
   int n_sms = 0;
   std::vector<std::unique_ptr<insem_cuda_solver>> members;  // null after remove()
   std::vector<char> prepared;
@@ -128,7 +135,6 @@ class Batch {
   cudaGraphExec_t graph = nullptr;
   // device tables of the current composition
   std::vector<DevClass> dclasses;
-  DeviceBuffer<int32_t> queues;
   DeviceBuffer<HaloSeg> dhalo_segs[3];
   DeviceBuffer<int2> dhalo_items[3];
   int32_t n_halo_items[3] = {0, 0, 0};

@@ -275,7 +275,6 @@ struct TileLayout {
 };
 
 // Mode-dependent completion of a point (solver.cpp:924-944 fused):
-// Mode-dependent completion of a point (solver.cpp:924-944 fused):
 //   normal: v = v_half + dt/2 a; u' = u + dt v + dt^2/2 a; v' = v + dt/2 a
 //   final:  v = v_half + dt/2 a; u' = u                      (state complete)
 //   init:   v unchanged;         u' = u                      (step 0)
@@ -329,15 +328,16 @@ static __global__ void predictor_inplace_kernel(float* __restrict__ u, float* __
   }
 }
 
-// One tile of the fused step (the whole CTA).  `bar` is an initialised
-// mbarrier whose next phase to complete has parity `phase`.  Returns false
-// (after recording the error) if the tile's bulk copies did not arrive
-// within the wait limit.
+// One tile of the fused step (the whole CTA).  `thp` is the tile's header
+// (entry `tile` of the domain's tile table, or a copy of it).  `bar` is an
+// initialised mbarrier whose next phase to complete has parity `phase`.
+// Returns false (after recording the error) if the tile's bulk copies did
+// not arrive within the wait limit.
 template <int NG, int KIND, bool EL, int M>
 __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledDev& td, const StepScalars& sc,
                                                StepState* __restrict__ st, double* __restrict__ epartial,
-                                               int32_t tile, const TileLayout& L, unsigned char* smem_raw,
-                                               uint64_t* bar, uint32_t phase) {
+                                               int32_t tile, const TileHdr* thp, const TileLayout& L,
+                                               unsigned char* smem_raw, uint64_t* bar, uint32_t phase) {
   using Cfg = TileCfg<NG>;
   using CE = ElemCfg<NG, KIND, EL, M>;
   constexpr int NC = CE::NC;
@@ -359,7 +359,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   float* sax = reinterpret_cast<float*>(smem_raw + L.ax);  // [TE][4][AXS] axis terms
   const int tp_cap = L.tp_cap, nc_cap = L.nc_cap;
 
-  const TileHdr th = td.tiles[tile];
+  const TileHdr th = *thp;
   const int tid = threadIdx.x;
   const int nthreads = blockDim.x;  // (tile elements) x NG
   const int mode = st->mode;
@@ -396,12 +396,14 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   const bool active = el < th.ne;
   uint32_t dsc[NG];
   float ec0 = 0.0f, ec1 = 0.0f;  // the element's material coefficients
+  bool axial = false;             // axisymmetric element on the axis (GLJ basis in xi)
   if (active) {
     const uint32_t* gdesc = td.sdesc + static_cast<size_t>(th.be0 + el) * CS + i;
 #pragma unroll
     for (int j = 0; j < NG; ++j) dsc[j] = gdesc[j * NG];
     ec0 = blk.coef0[th.be0 + el];
     if constexpr (EL) ec1 = blk.coef1[th.be0 + el];
+    if constexpr (AXI) axial = blk.axial[th.be0 + el] != 0;
   }
   // halo tile points, gathered while the bulk copies are in flight
   for (int t = tid; t < th.ntp - th.nc; t += nthreads) {
@@ -462,7 +464,6 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   __syncthreads();
 
   // 3. derivatives and fluxes, one column per thread
-  const bool axial = AXI && active && blk.axial[th.be0 + el] != 0;
   float dxr[NG], dxc[NG], w2c[NG];  // Dx row i, Dx column i, w_i w_j
 #pragma unroll
   for (int l = 0; l < NG; ++l) {
@@ -615,7 +616,14 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     }
   }
 
-  // 5. local assembly in the reference's slot order, halo staging
+  // 5. local assembly in the reference's slot order, halo staging.  This
+  //    thread's first halo entry (step 6) is fetched now, so that its index
+  //    loads complete during the assembly phases.
+  int32_t hs_first = 0, hd_first = 0;
+  if (tid < th.nhs) {
+    hs_first = td.hs_slot[th.hs_off + tid];
+    hd_first = td.hs_dst[th.hs_off + tid];
+  }
   float* stage = su;
   if (active) {
 #pragma unroll
@@ -647,8 +655,8 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 
   // 6. halo contributions out, each to its place in its halo point's list
   for (int q = tid; q < th.nhs; q += nthreads) {
-    const int32_t ls = td.hs_slot[th.hs_off + q];
-    const int32_t dst = td.hs_dst[th.hs_off + q];
+    const int32_t ls = q == tid ? hs_first : td.hs_slot[th.hs_off + q];
+    const int32_t dst = q == tid ? hd_first : td.hs_dst[th.hs_off + q];
     const int e = ls / NPE, k = ls - e * NPE;
     float val[NC];
 #pragma unroll
@@ -737,7 +745,8 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
     mbar_init(bar + 1, 1);
   }
   __syncthreads();
-  tile_step_body<NG, KIND, EL, M>(blk, td, sc, st, epartial, tile0 + blockIdx.x, L, smem_raw, bar, 0u);
+  const int32_t tile = tile0 + blockIdx.x;
+  tile_step_body<NG, KIND, EL, M>(blk, td, sc, st, epartial, tile, td.tiles + tile, L, smem_raw, bar, 0u);
 }
 
 // Tiles of many solves in one launch.  A segment is one block of one
@@ -748,60 +757,59 @@ struct TileSeg {
   StepScalars sc;
   StepState* st;
   double* epartial;     // the domain's tile partials
-  int32_t tile0;        // the block's first tile in the domain's tile table
 };
 
-// Work items (segment, tile within the block) come from a device queue:
-// `queue` is zeroed by the step's first kernel.  The grid has one CTA per
-// item.  A CTA claims items until it holds one of a running solve (items of
-// finished solves are skipped), finishes that tile and exits.  (CTAs that
-// loop over items measured slower: the loop keeps about 40 more registers
-// per thread live, which costs resident CTAs per SM.)  One shared memory
-// layout serves the class (sized for its largest tile).
+// One work item of a batched tile launch: a tile of one segment, with a copy
+// of its header and its solve's step state, so that a CTA needs one load of
+// its item before it can read the segment and the state (in parallel) and
+// issue the tile's bulk copies.
+struct __align__(16) TileItem {
+  TileHdr th;             // the tile's header (entry `tile` of the domain's table)
+  const StepState* st;    // the segment's solve
+  int32_t seg;            // segment index
+  int32_t tile;           // tile index in the domain's table (energy partials)
+};
+static_assert(sizeof(TileItem) == 64, "TileItem is loaded as 16 words");
+
+// One CTA per work item (CTA b takes item b).  Items of solves past their
+// last step (idle) are skipped: the CTA exits.  (CTAs that loop over items
+// measured slower: the loop keeps about 40 more registers per thread live,
+// which costs resident CTAs per SM.)  One shared memory layout serves the
+// class (sized for its largest tile).
 template <int NG, int KIND, bool EL, int M>
 static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
-    tile_batch_kernel(const TileSeg* __restrict__ segs, const int2* __restrict__ items, int32_t n_items,
-                      int32_t* __restrict__ queue, TileLayout L) {
+    tile_batch_kernel(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items, TileLayout L) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
-  __shared__ __align__(16) TileSeg s_seg;  // the item's segment, read by the body from shared memory
-  __shared__ int32_t s_item, s_segi, s_tile, s_idle;
+  __shared__ __align__(16) TileSeg s_seg;   // the item's segment, read by the body from shared memory
+  __shared__ __align__(16) TileItem s_it;
+  __shared__ int32_t s_idle, s_parity;
   static_assert(sizeof(TileSeg) % 4 == 0, "TileSeg is copied as 32-bit words");
+  if (threadIdx.x < 16)
+    reinterpret_cast<uint32_t*>(&s_it)[threadIdx.x] = reinterpret_cast<const uint32_t*>(items + blockIdx.x)[threadIdx.x];
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
   }
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const int32_t w = atomicAdd(queue, 1);
-      s_item = w;
-      if (w < n_items) {
-        const int2 it = items[w];
-        s_segi = it.x;
-        s_tile = it.y;
-      }
-    }
-    __syncthreads();
-    if (s_item >= n_items) return;
-    {
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(segs + s_segi);
-      uint32_t* dst = reinterpret_cast<uint32_t*>(&s_seg);
-      for (int q = threadIdx.x; q < static_cast<int>(sizeof(TileSeg) / 4); q += blockDim.x) dst[q] = src[q];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      s_idle = s_seg.st->mode == kModeIdle;
-      if (s_seg.st->parity) {
-        const float* cur = s_seg.td.u_cur;
-        s_seg.td.u_cur = s_seg.td.u_nxt;
-        s_seg.td.u_nxt = const_cast<float*>(cur);
-      }
-    }
-    __syncthreads();
-    if (!s_idle) break;
-    __syncthreads();  // the next claim rewrites the item and the segment
+  __syncthreads();
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(segs + s_it.seg);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&s_seg);
+    for (int q = threadIdx.x; q < static_cast<int>(sizeof(TileSeg) / 4); q += blockDim.x) dst[q] = src[q];
   }
-  tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial, s_seg.tile0 + s_tile, L,
+  if (threadIdx.x == blockDim.x - 1) {
+    s_idle = s_it.st->mode == kModeIdle;
+    s_parity = s_it.st->parity;
+  }
+  __syncthreads();
+  if (s_idle) return;
+  if (threadIdx.x == 0 && s_parity) {
+    const float* cur = s_seg.td.u_cur;
+    s_seg.td.u_cur = s_seg.td.u_nxt;
+    s_seg.td.u_nxt = const_cast<float*>(cur);
+  }
+  __syncthreads();
+  tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial, s_it.tile, &s_it.th, L,
                                   smem_raw, bar, 0u);
 }
 
@@ -1153,11 +1161,9 @@ static __global__ void __launch_bounds__(kReduceThreads) energy_batch_kernel(con
 }
 
 // First kernel of a batched step: every solve's step counter, buffer parity
-// and mode (final on its last step, idle after it), and the tile queues reset.
-static __global__ void batch_begin_kernel(StepState* const* __restrict__ sts, int32_t n, int32_t* __restrict__ queues,
-                                          int32_t n_queues) {
+// and mode (final on its last step, idle after it).
+static __global__ void batch_begin_kernel(StepState* const* __restrict__ sts, int32_t n) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n_queues) queues[i] = 0;
   if (i < n) {
     StepState* s = sts[i];
     if (s->step >= s->last_step) {

@@ -534,6 +534,7 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
   // 7. uploads
   sdesc.upload(desc);
   tiles.upload(hdr);
+  host_tiles = std::move(hdr);
   halo_tp.upload(htp.empty() ? std::vector<int32_t>{0} : htp);
   hs_slot.upload(hslot.empty() ? std::vector<int32_t>{0} : hslot);
   hs_dst.upload(hdst.empty() ? std::vector<int32_t>{0} : hdst);

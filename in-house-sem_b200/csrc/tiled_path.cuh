@@ -42,6 +42,7 @@ class TiledDomain {
   // device data
   DeviceBuffer<uint32_t> sdesc;
   DeviceBuffer<TileHdr> tiles;
+  std::vector<TileHdr> host_tiles;  // the same headers on the host (the batched tile items copy them)
   DeviceBuffer<int32_t> halo_tp, hs_slot, hs_dst, mdst_off, mdst, cs_slot, cs_idx, cs_row;
   DeviceBuffer<float> cval, hbuf, mass, inv_mass;
   DeviceBuffer<float> u0, u1, v, a, vn;
@@ -95,9 +96,7 @@ struct TileBatchLaunch {
   int kind = 0, m = 0;
   bool elastic = false;
   const TileSeg* segs = nullptr;
-  const int2* items = nullptr;
-  int32_t n_items = 0;
-  int32_t* queue = nullptr;
+  const TileItem* items = nullptr;
   int te = 0;      // elements per tile of the class (CTA size tile_threads(te, ngll))
   TileLayout L{};  // the class layout; its total is the dynamic shared memory
   uint32_t smem = 0;
@@ -127,7 +126,7 @@ int tile_batch_cfg(const TileBatchLaunch& a, bool launch) {
       return nb;
     }
     INSEM_REQUIRE(a.te >= 1 && a.te <= TileCfg<NG>::TE, INSEM_CUDA_ERR_INVALID, "tile elements out of range");
-    kernel<<<a.grid, tile_threads(a.te, NG), a.smem, a.stream>>>(a.segs, a.items, a.n_items, a.queue, a.L);
+    kernel<<<a.grid, tile_threads(a.te, NG), a.smem, a.stream>>>(a.segs, a.items, a.L);
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess)
       throw Error(INSEM_CUDA_ERR_CUDA, "batched tile kernel launch (ngll " + std::to_string(NG) + ", kind " +

@@ -97,7 +97,7 @@ class Time(C.Structure):
 
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("use_graphs", C.c_int32), ("path", C.c_int32),
-                ("tile_elements", C.c_int32), ("check_finite", C.c_int32)]
+                ("tile_elements", C.c_int32), ("check_finite", C.c_int32), ("tile_streams", C.c_int32)]
 
 
 _lib = None

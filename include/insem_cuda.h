@@ -216,6 +216,7 @@ typedef struct insem_cuda_options {
   int32_t path;            /* 0 default; 1 plain two-pass (element forces -> CSR assemble); 2 tiled fused */
   int32_t tile_elements;   /* tiled path: elements per tile (0 = autotuned) */
   int32_t check_finite;    /* 1: check fields for NaN/Inf at every advance() end (default 1) */
+  int32_t tile_streams;    /* batches: streams the tile launches of a step spread over (0 = default 2, at most 8) */
 } insem_cuda_options;
 
 /* ------------------------------------------------- per-block kernel seam */

@@ -39,11 +39,13 @@ def _check_golden(case, prob, s, z):
         assert np.abs(e[:, 1:] - ge[:, 1:]).max() <= 1e-9 * np.abs(ge[:, 1:]).max()
 
 
-@pytest.mark.parametrize("graphs", [True, False])
-def test_batch_of_all_cases_matches_reference(pkg, graphs):
+@pytest.mark.parametrize("graphs,streams", [(True, 0), (False, 0), (True, 1), (True, 8)])
+def test_batch_of_all_cases_matches_reference(pkg, graphs, streams):
+    """Every case in one batch; the tile classes on the default number of
+    streams, on one stream and on eight (results do not depend on it)."""
     from insem_b200 import Batch
 
-    with Batch(use_graphs=graphs) as b:
+    with Batch(use_graphs=graphs, tile_streams=streams) as b:
         entries = []
         for case in RUN_CASES:
             z = golden(case)
