@@ -64,6 +64,21 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback"
 
 
+def traffic(name: str, algorithmic_bytes: int):
+    """DRAM bytes (read + write) of the roofline's kernels, from the ncu capture
+    recorded in data/dram_traffic_b200.json for this workload: the captured
+    DRAM bytes per algorithmic byte, times this run's algorithmic bytes (the
+    capture is a smaller case of the same kernels; DRAM bytes grow with the
+    elements and points processed)."""
+    p = REPO / "in-house-sem_b200" / "data" / "dram_traffic_b200.json"
+    if not p.exists():
+        return None, None
+    rec = json.loads(p.read_text()).get(name)
+    if not rec:
+        return None, None
+    return rec["dram_per_algorithmic_byte"] * algorithmic_bytes, rec["source"]
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons while running."""
 
@@ -288,11 +303,12 @@ def bench_config3(args, world, rank, device, pg, headline: bool) -> dict:
     hbm, how = peaks()
     b_step = prob.algorithmic_bytes_per_step()
     achieved = b_step / (ms * 1e-3 / steps) / 1e9
+    dram, dram_src = traffic("config3_step", b_step)
     out = {"value": replica_value(world, points * steps, ms), "ms_per_step": ms / steps, "steps": steps,
            "workload": f"config3 coupled 2D Cartesian {args.nx}x{args.nx} order 5 (water over 8 curved elastic layers)",
            "points": points, "elements": prob.n_elements_total(), "setup_seconds": round(setup_s, 1),
            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                        "traffic": None, "kernel": "whole step (all kernels of one step)",
+                        "traffic": dram, "traffic_source": dram_src, "kernel": "whole step (all kernels of one step)",
                         "algorithmic_bytes_per_step": b_step, "peak_source": how},
            "kernels_per_step": kps, "clocks": clocks.summary()}
     if headline and not args.no_e2e:
@@ -339,6 +355,8 @@ def build_config4(args, device):
     t0 = time.perf_counter()
     table = None if args.no_autotune else autotune.tune_batched([q for _, q in probs], device=device)
     tune_s = time.perf_counter() - t0
+    if table and args.save_tiles:
+        autotune.save(table, args.save_tiles)
     out = [(p, prob, pkg.Solver(prob, device=device, use_graphs=not args.no_graphs)) for p, prob in probs]
     return out, {"classes": autotune.summary(table), "seconds": round(tune_s, 1)} if table else None
 
@@ -371,7 +389,7 @@ def bench_config4(args, world, rank, device, pg) -> dict:
     plain_value = replica_value(world, plain_updates, plain_ms)
 
     # batched
-    batch = pkg.Batch(device=device, use_graphs=not args.no_graphs)
+    batch = pkg.Batch(device=device, use_graphs=not args.no_graphs, tile_streams=args.tile_streams)
     members = [batch.adopt(s) for _, _, s in models]
     batch.advance(args.warmup)
     barrier(pg, device)
@@ -409,6 +427,7 @@ def bench_config4(args, world, rank, device, pg) -> dict:
     per_step_tile_s = tile_ms * 1e-3 / args.profile_steps
     achieved = tile_bytes / per_step_tile_s / 1e9
     step_achieved = b_step / (ms * 1e-3 / args.steps) / 1e9
+    dram, dram_src = traffic("batched_tiles", tile_bytes)
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -424,7 +443,8 @@ def bench_config4(args, world, rank, device, pg) -> dict:
         "batched_over_plain": value / plain_value,
         "e2e": line_e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "kernel": "tile_batch_kernel (all tile classes of one batched step)",
+                     "traffic": dram, "traffic_source": dram_src,
+                     "kernel": "tile_batch_kernel (all tile classes of one batched step)",
                      "algorithmic_bytes_per_launch_group": tile_bytes, "ms_per_launch_group": tile_ms / args.profile_steps,
                      "tile_share_of_step": tile_ms / step_ms if step_ms > 0 else None, "peak_source": how},
         "step_roofline": {"achieved": step_achieved, "frac": step_achieved / hbm, "algorithmic_bytes_per_step": b_step},
@@ -531,6 +551,10 @@ def main():
     ap.add_argument("--config3-steps", type=int, default=200, help="steps of the config3 sub-run")
     ap.add_argument("--no-config3", action="store_true", help="skip the config3 sub-run")
     ap.add_argument("--no-autotune", action="store_true", help="batched workload: keep the default tile sizes")
+    ap.add_argument("--tile-streams", type=int, default=0,
+                    help="batched workload: streams the tile launches of a step spread over (0 = library default)")
+    ap.add_argument("--save-tiles", default=None,
+                    help="batched workload: write the tuned tile table (JSON, autotune.load format) here")
     ap.add_argument("--setup-threads", type=int, default=16,
                     help="batched workload: host threads building the models and their stable time steps")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving stream")
