@@ -93,11 +93,13 @@ void Solver::batch_collect(BatchTables& T) {
       c.te = std::max(c.te, t.te);
       c.tp_cap = std::max(c.tp_cap, t.tp_cap);
       c.nc_cap = std::max(c.nc_cap, t.nc_cap);
+      c.rank_cap = std::max(c.rank_cap, t.rank_cap);
       const int32_t seg = static_cast<int32_t>(c.segs.size());
       c.segs.push_back(sg);
       for (int k = 0; k < bt.ntiles; ++k) {
         TileItem it{};
         it.th = t.host_tiles[bt.tile0 + k];
+        it.halo_tp = sg.td.halo_tp + it.th.hl_off;
         it.st = st;
         it.seg = seg;
         it.tile = bt.tile0 + k;
@@ -327,7 +329,7 @@ void Batch::rebuild() {
     d.items.upload_async(c.items, stream);
     d.n_items = static_cast<int32_t>(c.items.size());
     d.te = c.te;
-    d.L = TileLayout::make(c.ngll, c.ncomp, c.kind, c.elastic, c.te, c.tp_cap, c.nc_cap);
+    d.L = TileLayout::make(c.ngll, c.ncomp, c.kind, c.elastic, c.te, c.tp_cap, c.nc_cap, c.rank_cap);
     TileBatchLaunch a;
     a.te = c.te;
     a.kind = c.kind;

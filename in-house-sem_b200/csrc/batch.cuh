@@ -39,7 +39,7 @@ struct StreamSeg {
 struct TileClass {
   int ngll = 0, kind = 0, m = 0, ncomp = 0;
   bool elastic = false;
-  int tp_cap = 0, nc_cap = 0, te = 0;  // largest tile of the class
+  int tp_cap = 0, nc_cap = 0, te = 0, rank_cap = 1;  // largest tile of the class
   std::vector<TileSeg> segs;
   std::vector<TileItem> items;
 };

@@ -98,6 +98,7 @@ constexpr uint32_t kSlotPointMask = 0xffffu;      // tile point index
 constexpr int kSlotRankShift = 16;                // local assembly rank (0..254)
 constexpr uint32_t kSlotRankNone = 0xffu;          // not assembled in the tile
 constexpr uint32_t kSlotConstrained = 1u << 24;   // value from the constrained-slot list
+constexpr uint32_t kSlotLast = 1u << 25;          // the highest rank of its (complete) point
 
 struct TileHdr {
   int32_t be0;     // first element of the tile (block-local, tile order)
@@ -212,15 +213,20 @@ constexpr uint32_t kBulkWaitLimit = 1u << 22;
 // threads into the u region after the complete points (at index
 // roundup(nc, 4) on).  The material coefficients (one pair per element) and
 // the slot descriptors (which each column thread keeps in registers) are read
-// from global memory by the threads that use them.
+// from global memory by the threads that use them.  `pl` holds, for every
+// complete point, the staging places of its contributions in rank order
+// (`rs` entries per point, uint16).
 struct TileLayout {
-  uint32_t bar, metric, wr, hoop, r, u, v, im, tf, su, sfx, ax, total;
-  int32_t tp_cap, nc_cap, ms, cs, row;
+  uint32_t bar, metric, wr, hoop, r, u, v, im, pl, su, sfx, ax, total;
+  int32_t tp_cap, nc_cap, ms, cs, row, rs;
   int32_t late;  // 1: v and 1/M arrive by a second copy into the element-data region
 
   __host__ __device__ static uint32_t up16(uint32_t x) { return (x + 15u) & ~15u; }
-  __host__ __device__ static TileLayout make(int ng, int nc, int kind, bool elastic, int te, int tp_cap, int nc_cap) {
+  // rs: the most contributions one complete point of the class's tiles has
+  __host__ __device__ static TileLayout make(int ng, int nc, int kind, bool elastic, int te, int tp_cap, int nc_cap,
+                                            int rs) {
     TileLayout L{};
+    L.rs = (rs + 3) & ~3;  // a point's list is read four entries (8 bytes) at a time
     const int npe = ng * ng;
     L.cs = (npe + 3) & ~3;
     L.ms = kind == INSEM_RECT ? 4 : kind == INSEM_AFFINE ? 8 : (kind == INSEM_AXISYM ? 4 : 5) * L.cs;
@@ -239,10 +245,11 @@ struct TileLayout {
     if (axi) o = up16(o + 4u * te * L.cs);
     L.r = o;
     if (axi) o = up16(o + 4u * te * L.cs);
-    // The element data [metric, elem_end) is last read by the fluxes.  The
-    // f_xi rows (written after the fluxes, read by the divergence) and then
-    // the assembly target with v and 1/M (copied in after the divergence)
-    // reuse that region when it is large enough.
+    // The element data [metric, elem_end) is last read by the fluxes.  Then
+    // that region takes, when it is large enough, the f_xi rows (written
+    // after the fluxes, read by the divergence) and beside them v and 1/M
+    // (copied in after the fluxes); the point lists (written after the
+    // divergence) take the place of the f_xi rows.
     const uint32_t elem = o - L.metric;
     L.u = o;
     o = up16(o + 4u * nc * tp_cap);
@@ -260,13 +267,15 @@ struct TileLayout {
       L.sfx = o;
       o += sfx_b;
     }
-    const uint32_t tf_b = up16(4u * nc * tp_cap), v_b = up16(4u * nc * nc_cap), im_b = up16(4u * nc_cap);
-    L.late = tf_b + v_b + im_b <= elem ? 1 : 0;
+    const uint32_t pl_b = up16(2u * L.rs * nc_cap), v_b = up16(4u * nc * nc_cap), im_b = up16(4u * nc_cap);
+    const uint32_t sfx_in = L.sfx == L.metric ? sfx_b : 0u;  // f_xi rows inside the element data
+    const uint32_t head = pl_b > sfx_in ? pl_b : sfx_in;
+    L.late = head + v_b + im_b <= elem ? 1 : 0;
     uint32_t p = L.late ? L.metric : o;
-    L.tf = p;
-    L.v = p + tf_b;
-    L.im = p + tf_b + v_b;
-    if (!L.late) o += tf_b + v_b + im_b;
+    L.pl = p;
+    L.v = p + (L.late ? head : pl_b);
+    L.im = L.v + v_b;
+    if (!L.late) o += pl_b + v_b + im_b;
     L.ax = o;
     if (axi) o = up16(o + 4u * te * 4 * ((ng + 3) & ~3));
     L.total = o;
@@ -329,7 +338,9 @@ static __global__ void predictor_inplace_kernel(float* __restrict__ u, float* __
 }
 
 // One tile of the fused step (the whole CTA).  `thp` is the tile's header
-// (entry `tile` of the domain's tile table, or a copy of it).  `bar` is an
+// (entry `tile` of the domain's tile table, or a copy of it).  `g_first`, if
+// not negative, is this thread's first halo tile point (its halo_tp entry),
+// already loaded.  `bar` is an
 // initialised mbarrier whose next phase to complete has parity `phase`.
 // Returns false (after recording the error) if the tile's bulk copies did
 // not arrive within the wait limit.
@@ -337,7 +348,8 @@ template <int NG, int KIND, bool EL, int M>
 __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledDev& td, const StepScalars& sc,
                                                StepState* __restrict__ st, double* __restrict__ epartial,
                                                int32_t tile, const TileHdr* thp, const TileLayout& L,
-                                               unsigned char* smem_raw, uint64_t* bar, uint32_t phase) {
+                                               unsigned char* smem_raw, uint64_t* bar, uint32_t phase,
+                                               int32_t g_first = -1) {
   using Cfg = TileCfg<NG>;
   using CE = ElemCfg<NG, KIND, EL, M>;
   constexpr int NC = CE::NC;
@@ -353,7 +365,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   float* tu = reinterpret_cast<float*>(smem_raw + L.u);    // [NC][tp_cap]
   float* s_v = reinterpret_cast<float*>(smem_raw + L.v);   // [NC][nc_cap]
   float* s_im = reinterpret_cast<float*>(smem_raw + L.im); // [nc_cap]
-  float* tf = reinterpret_cast<float*>(smem_raw + L.tf);   // [NC][tp_cap]
+  uint16_t* pl = reinterpret_cast<uint16_t*>(smem_raw + L.pl);  // [nc_cap][rs] staging places, rank order
   float* su = reinterpret_cast<float*>(smem_raw + L.su);   // [TE][NC][NG][ROW] field rows, later staging
   float* sfx = reinterpret_cast<float*>(smem_raw + L.sfx); // [TE][NC][NG][ROW] f_xi rows
   float* sax = reinterpret_cast<float*>(smem_raw + L.ax);  // [TE][4][AXS] axis terms
@@ -407,7 +419,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   }
   // halo tile points, gathered while the bulk copies are in flight
   for (int t = tid; t < th.ntp - th.nc; t += nthreads) {
-    const int32_t g = td.halo_tp[th.hl_off + t];
+    const int32_t g = (t == tid && g_first >= 0) ? g_first : td.halo_tp[th.hl_off + t];
 #pragma unroll
     for (int c = 0; c < NC; ++c) tu[c * tp_cap + nc4 + t] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
   }
@@ -547,6 +559,18 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     }
   }
   __syncthreads();  // the element data is dead: the f_xi rows may overwrite it
+  // v and 1/M of the complete points, into the element-data region beside
+  // the f_xi rows, while the divergence runs
+  if (L.late && tid == 0) {
+    fence_proxy_async_smem();
+    mbar_expect_tx(bar + 1, nc4 > 0 ? 4u * nc4 * (NC + 1) : 0u);
+    if (nc4 > 0) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        bulk_load(s_v + c * nc_cap, td.v + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar + 1);
+      bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar + 1);
+    }
+  }
   if (active && NC != 3) {
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
@@ -603,55 +627,30 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   }
   __syncthreads();  // su is reused below as halo staging; the f_xi rows are dead
 
-  // v and 1/M of the complete points, into the element-data region behind the
-  // assembly target, while the assembly runs
-  if (L.late && tid == 0) {
-    fence_proxy_async_smem();
-    mbar_expect_tx(bar + 1, nc4 > 0 ? 4u * nc4 * (NC + 1) : 0u);
-    if (nc4 > 0) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c)
-        bulk_load(s_v + c * nc_cap, td.v + static_cast<size_t>(c) * td.ng + th.cbeg, 4u * nc4, bar + 1);
-      bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar + 1);
-    }
-  }
-
-  // 5. local assembly in the reference's slot order, halo staging.  This
-  //    thread's first halo entry (step 6) is fetched now, so that its index
-  //    loads complete during the assembly phases.
+  // 5. every slot's contribution to the staging area; each complete point's
+  //    slots listed by rank (their sum is formed in step 7, in rank order,
+  //    which is the reference's ascending slot order).  This thread's first
+  //    halo entry (step 6) is fetched now, so that its index loads complete
+  //    meanwhile.
   int32_t hs_first = 0, hd_first = 0;
   if (tid < th.nhs) {
     hs_first = td.hs_slot[th.hs_off + tid];
     hd_first = td.hs_dst[th.hs_off + tid];
   }
-  float* stage = su;
+  float* stage = su;  // [te][NC][NPE]
+  const int rs = L.rs;
   if (active) {
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
+      const int base = el * NC * NPE + j * NG + i;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) stage[base + c * NPE] = fo[c][j];
       const uint32_t rank = (dsc[j] >> kSlotRankShift) & 0xffu;
-      if (rank == kSlotRankNone || (dsc[j] & kSlotConstrained)) {
-#pragma unroll
-        for (int c = 0; c < NC; ++c) stage[(el * NC + c) * NPE + j * NG + i] = fo[c][j];
-      }
+      if (rank != kSlotRankNone)
+        pl[(dsc[j] & kSlotPointMask) * rs + rank] = static_cast<uint16_t>(base | ((dsc[j] & kSlotLast) ? 0x8000 : 0));
     }
   }
-  for (int r = 0; r <= th.maxrank; ++r) {
-    if (active) {
-#pragma unroll
-      for (int j = 0; j < NG; ++j) {
-        const uint32_t rank = (dsc[j] >> kSlotRankShift) & 0xffu;
-        if (rank == static_cast<uint32_t>(r) && !(dsc[j] & kSlotConstrained)) {
-          const int p = dsc[j] & kSlotPointMask;
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            float* t = tf + c * tp_cap + p;
-            *t = (r == 0) ? fadd(0.0f, fo[c][j]) : fadd(*t, fo[c][j]);
-          }
-        }
-      }
-    }
-    __syncthreads();
-  }
+  __syncthreads();
 
   // 6. halo contributions out, each to its place in its halo point's list
   for (int q = tid; q < th.nhs; q += nthreads) {
@@ -688,10 +687,34 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   for (int t = tid; t < th.nc; t += nthreads) {
     const int32_t g = th.cbeg + t;
     const float im = s_im[t];
+    // the point's force: its contributions added in rank order, 0 + f_0
+    // first.  Four list entries come in one load; the values of the valid
+    // ones (up to the entry flagged last) load together, then add in order.
+    float fsum[NC] = {};
+    bool more = true;
+    for (int r0 = 0; more && r0 < rs; r0 += 4) {
+      const uint2 w = *reinterpret_cast<const uint2*>(pl + t * rs + r0);
+      const uint32_t e[4] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16};
+      bool valid[4];
+      valid[0] = true;
+#pragma unroll
+      for (int k = 1; k < 4; ++k) valid[k] = valid[k - 1] && !(e[k - 1] & 0x8000u);
+      float x[4][NC];
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) x[k][c] = valid[k] ? stage[(e[k] & 0x7fffu) + c * NPE] : 0.0f;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+#pragma unroll
+        for (int c = 0; c < NC; ++c)
+          if (valid[k]) fsum[c] = (r0 + k == 0) ? fadd(0.0f, x[k][c]) : fadd(fsum[c], x[k][c]);
+      more = valid[3] && !(e[3] & 0x8000u);
+    }
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       const size_t gi = static_cast<size_t>(c) * td.ng + g;
-      const float f = tf[c * tp_cap + t];
+      const float f = fsum[c];
       const float a = fmul(f, im);
       const float u = tu[c * tp_cap + t];
       float u_out, v_state, v_n;
@@ -760,16 +783,19 @@ struct TileSeg {
 };
 
 // One work item of a batched tile launch: a tile of one segment, with a copy
-// of its header and its solve's step state, so that a CTA needs one load of
-// its item before it can read the segment and the state (in parallel) and
-// issue the tile's bulk copies.
+// of its header, its solve's step state and its halo point list, so that a
+// CTA needs one load of its item before it can read the segment, the state
+// and its first halo tile points (in parallel) and issue the tile's bulk
+// copies.
 struct __align__(16) TileItem {
-  TileHdr th;             // the tile's header (entry `tile` of the domain's table)
-  const StepState* st;    // the segment's solve
-  int32_t seg;            // segment index
-  int32_t tile;           // tile index in the domain's table (energy partials)
+  TileHdr th;               // the tile's header (entry `tile` of the domain's table)
+  const StepState* st;      // the segment's solve
+  int32_t seg;              // segment index
+  int32_t tile;             // tile index in the domain's table (energy partials)
+  const int32_t* halo_tp;   // the tile's halo tile points (domain halo_tp + th.hl_off)
+  int64_t pad;
 };
-static_assert(sizeof(TileItem) == 64, "TileItem is loaded as 16 words");
+static_assert(sizeof(TileItem) == 80, "TileItem is loaded as 20 words");
 
 // One CTA per work item (CTA b takes item b).  Items of solves past their
 // last step (idle) are skipped: the CTA exits.  (CTAs that loop over items
@@ -785,13 +811,15 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   __shared__ __align__(16) TileItem s_it;
   __shared__ int32_t s_idle, s_parity;
   static_assert(sizeof(TileSeg) % 4 == 0, "TileSeg is copied as 32-bit words");
-  if (threadIdx.x < 16)
+  if (threadIdx.x < 20)
     reinterpret_cast<uint32_t*>(&s_it)[threadIdx.x] = reinterpret_cast<const uint32_t*>(items + blockIdx.x)[threadIdx.x];
   if (threadIdx.x == 0) {
     mbar_init(&bar[0], 1);
     mbar_init(&bar[1], 1);
   }
   __syncthreads();
+  // this thread's first halo tile point, loaded beside the segment and the state
+  const int32_t g_first = static_cast<int>(threadIdx.x) < s_it.th.ntp - s_it.th.nc ? s_it.halo_tp[threadIdx.x] : -1;
   {
     const uint32_t* src = reinterpret_cast<const uint32_t*>(segs + s_it.seg);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&s_seg);
@@ -810,7 +838,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   }
   __syncthreads();
   tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial, s_it.tile, &s_it.th, L,
-                                  smem_raw, bar, 0u);
+                                  smem_raw, bar, 0u, g_first);
 }
 
 // ------------------------------------------------------------ halo kernel

@@ -148,7 +148,7 @@ int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp) {
     const int side = static_cast<int>(std::ceil(std::sqrt(static_cast<double>(te))));
     const int nc = te * q * q;
     const int tp = nc + 4 * side * q + 4;
-    const TileLayout L = TileLayout::make(ngll, ncomp, kind, elastic, te, (tp + 3) & ~3, (nc + 3) & ~3);
+    const TileLayout L = TileLayout::make(ngll, ncomp, kind, elastic, te, (tp + 3) & ~3, (nc + 3) & ~3, 4);
     const int ctas = std::min({(228 * 1024) / (static_cast<int>(L.total) + 1024), 2048 / tile_threads(te, ngll), 32});
     if (ctas < 1) continue;
     const double halo = static_cast<double>(tp - nc) / tp;                 // points shared with other tiles
@@ -439,6 +439,7 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
             INSEM_REQUIRE(p >= 0 && p < 65536, INSEM_CUDA_ERR_UNSUPPORTED, "tile has too many points");
             const uint32_t rank = owner[g] == t ? rank_of[s] : kSlotRankNone;
             dsc = static_cast<uint32_t>(p) | (rank << kSlotRankShift);
+            if (owner[g] == t && static_cast<int32_t>(rank) == t_off[g + 1] - t_off[g] - 1) dsc |= kSlotLast;
             if (owner[g] == t) {
               th.maxrank = std::max<int32_t>(th.maxrank, static_cast<int32_t>(rank));
             } else {
@@ -467,9 +468,11 @@ void TiledDomain::build(const insem_cuda_domain& d, int ngll, int te, const Spec
   n_cslots = static_cast<int32_t>(crow.size());
   tp_cap = 4;
   nc_cap = 4;
+  rank_cap = 1;
   for (const auto& th : hdr) {
     tp_cap = std::max(tp_cap, up4(th.nc) + th.ntp - th.nc);
     nc_cap = std::max(nc_cap, up4(th.nc));
+    rank_cap = std::max(rank_cap, th.maxrank + 1);
   }
   tp_cap = up4(tp_cap);  // keeps every component row of the staged u 16-byte aligned
 

@@ -29,6 +29,7 @@ class TiledDomain {
   // reference's point count.  Halo points are [n_complete, n_complete + n_halo).
   int medium = 0, ncomp = 1, m = 0, ng = 0, ng_ref = 0, npe = 0, n_elements = 0;
   int n_complete = 0, n_halo = 0, n_tiles = 0, tp_cap = 0, nc_cap = 0, n_hbuf = 0, n_cslots = 0;
+  int rank_cap = 1;  // the most contributions one complete point of a tile has
   int te = 0;  // elements per tile (CTAs of tile_threads(te, ngll) threads)
   bool weighted = false;
   std::vector<int32_t> perm;  // reference point -> device point
@@ -158,7 +159,7 @@ void launch_tiles_cfg(const TileLaunch& a) {
   if (b.ntiles == 0) return;
   auto go = [&](auto kernel, int nc) {
     INSEM_REQUIRE(d.te >= 1 && d.te <= TileCfg<NG>::TE, INSEM_CUDA_ERR_INVALID, "tile elements out of range");
-    const TileLayout L = TileLayout::make(NG, nc, b.kind, a.elastic, d.te, d.tp_cap, d.nc_cap);
+    const TileLayout L = TileLayout::make(NG, nc, b.kind, a.elastic, d.te, d.tp_cap, d.nc_cap, d.rank_cap);
     const size_t smem = L.total;
     // Opt in to this launch's dynamic shared memory (outside stream capture;
     // the first launch of every tile kernel happens in the uncaptured initial step).

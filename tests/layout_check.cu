@@ -57,18 +57,21 @@ int main() {
       for (int elastic = 0; elastic <= 1; ++elastic)
         for (int m = 0; m <= (kind == 3 ? 1 : 0); ++m) {
           const int nc = elastic ? (m == 1 ? 3 : 2) : 1;
-          for (int te = 1; te <= te_max(ng); ++te) {
+          for (int te = 1; te <= te_max(ng); ++te)
+          for (int rs = 1; rs <= 8; rs += 3) {
             // capacities as the tile builder bounds them: complete points plus a perimeter of halo points
             int side = 1;
             while (side * side < te) ++side;
             const int ncp = te * q * q, tp = ncp + 4 * side * q + 4;
             const int tp_cap = (tp + 3) & ~3, nc_cap = (ncp + 3) & ~3;
-            const TileLayout L = TileLayout::make(ng, nc, kind, elastic != 0, te, tp_cap, nc_cap);
+            const TileLayout L = TileLayout::make(ng, nc, kind, elastic != 0, te, tp_cap, nc_cap, rs);
             ++cases;
             const std::string id = "ng " + std::to_string(ng) + " kind " + std::to_string(kind) + " elastic " +
-                                   std::to_string(elastic) + " m " + std::to_string(m) + " te " + std::to_string(te);
+                                   std::to_string(elastic) + " m " + std::to_string(m) + " te " + std::to_string(te) +
+                                   " rs " + std::to_string(rs);
             const uint32_t offs[] = {L.bar, L.metric, L.wr, L.hoop, L.r,  L.u,  L.v,
-                                     L.im,  L.tf,     L.su, L.sfx,  L.ax, L.total};
+                                     L.im,  L.pl,     L.su, L.sfx,  L.ax, L.total};
+            if (te * nc * npe > 32768) return fail(id + ": staging places do not fit the point lists' 15 bits");
             for (uint32_t o : offs)
               if (o % 16u) return fail(id + ": offset " + std::to_string(o) + " not 16-byte aligned");
             const uint32_t rows = static_cast<uint32_t>(rows_elem_stride(ng, nc));
@@ -79,22 +82,21 @@ int main() {
             const Region u{"u", L.u, L.u + 4u * nc * tp_cap};
             const Region su{"field rows / staging", L.su, L.su + 4u * te * su_floats};
             const Region sfx{"xi-flux rows", L.sfx, L.sfx + 4u * te * rows};
-            const Region tf{"assembly target", L.tf, L.tf + 4u * nc * tp_cap};
+            const Region pl{"point lists", L.pl, L.pl + 2u * rs * nc_cap};
             const Region v{"v", L.v, L.v + 4u * nc * nc_cap};
             const Region im{"1/M", L.im, L.im + 4u * nc_cap};
             const Region ax{"axis terms", L.ax, L.ax + (kind == 3 ? 4u * te * 4 * ((ng + 3) & ~3) : 0u)};
             // phases 1-3a: copies land, rows are built, fluxes read the element data
             std::vector<Region> p1 = {bar, elem, u, su, ax};
             if (nc == 3) p1.push_back(sfx);  // three-component classes write their f_xi rows during the fluxes
-            // phases 3b-4: flux rows written and read; the element data is dead
-            std::vector<Region> p2 = {bar, u, su, ax, sfx};
-            // phases 5-7: assembly, halo staging (in su), completion of the points
-            std::vector<Region> p3 = {bar, u, su, tf, v, im};
+            // phases 3b-4: flux rows written and read; the element data is dead, and
+            // v and 1/M arrive (late copies) or are held
+            std::vector<Region> p2 = {bar, u, su, ax, sfx, v, im};
+            // phases 5-7: staging (in su), point lists, completion of the points
+            std::vector<Region> p3 = {bar, u, su, pl, v, im};
             if (!L.late) {
               p1.push_back(v);
               p1.push_back(im);
-              p2.push_back(v);
-              p2.push_back(im);
             }
             for (const auto* set : {&p1, &p2, &p3})
               for (std::size_t a = 0; a < set->size(); ++a) {
@@ -105,7 +107,7 @@ int main() {
               }
             auto inside = [&](const Region& r) { return r.beg >= elem.beg && r.end <= elem.end; };
             if (L.sfx == L.metric && !inside(sfx)) return fail(id + ": xi-flux rows overrun the element data");
-            if (L.late && !(inside(tf) && inside(v) && inside(im)))
+            if (L.late && !(inside(pl) && inside(v) && inside(im)))
               return fail(id + ": late regions overrun the element data");
           }
         }
