@@ -25,6 +25,8 @@
 // constant bank.  Every sum keeps the reference's operand order.
 #pragma once
 
+#include <cstddef>
+
 #include "element_ops.cuh"
 #include "step_kernels.cuh"
 
@@ -339,8 +341,8 @@ static __global__ void predictor_inplace_kernel(float* __restrict__ u, float* __
 
 // One tile of the fused step (the whole CTA).  `thp` is the tile's header
 // (entry `tile` of the domain's tile table, or a copy of it).  `g_first`, if
-// not negative, is this thread's first halo tile point (its halo_tp entry),
-// already loaded.  `bar` is an
+// not negative, is this thread's first halo tile point (halo_tp entry
+// blockDim.x - 1 - threadIdx.x), already loaded.  `bar` is an
 // initialised mbarrier whose next phase to complete has parity `phase`.
 // Returns false (after recording the error) if the tile's bulk copies did
 // not arrive within the wait limit.
@@ -374,6 +376,10 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   const TileHdr th = *thp;
   const int tid = threadIdx.x;
   const int nthreads = blockDim.x;  // (tile elements) x NG
+  // thread 0 issues the bulk copies; the halo tile points are gathered from
+  // the last thread down, so thread 0 has the fewest of them
+  const int issuer = 0;
+  const int tg = nthreads - 1 - tid;
   const int mode = st->mode;
   const int32_t step = st->step;
   const bool energy = (mode == kModeInit) ? (sc.energy_every > 0) : (sc.energy_every > 0 && step % sc.energy_every == 0);
@@ -381,7 +387,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 
   // 1. bulk copies of the tile's element data, slot descriptors and complete
   //    points (u; v and 1/M too unless they come late)
-  if (tid == 0) {
+  if (tid == issuer) {
     const uint32_t eb = 4u * th.ne;
     uint32_t total = eb * MS + eb * CS * (AXI ? 3 : 0);
     if (nc4 > 0) total += 4u * nc4 * (L.late ? NC : 2 * NC + 1);
@@ -418,8 +424,8 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     if constexpr (AXI) axial = blk.axial[th.be0 + el] != 0;
   }
   // halo tile points, gathered while the bulk copies are in flight
-  for (int t = tid; t < th.ntp - th.nc; t += nthreads) {
-    const int32_t g = (t == tid && g_first >= 0) ? g_first : td.halo_tp[th.hl_off + t];
+  for (int t = tg; t < th.ntp - th.nc; t += nthreads) {
+    const int32_t g = (t == tg && g_first >= 0) ? g_first : td.halo_tp[th.hl_off + t];
 #pragma unroll
     for (int c = 0; c < NC; ++c) tu[c * tp_cap + nc4 + t] = td.u_cur[static_cast<size_t>(c) * td.ng + g];
   }
@@ -561,7 +567,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
   __syncthreads();  // the element data is dead: the f_xi rows may overwrite it
   // v and 1/M of the complete points, into the element-data region beside
   // the f_xi rows, while the divergence runs
-  if (L.late && tid == 0) {
+  if (L.late && tid == issuer) {
     fence_proxy_async_smem();
     mbar_expect_tx(bar + 1, nc4 > 0 ? 4u * nc4 * (NC + 1) : 0u);
     if (nc4 > 0) {
@@ -637,14 +643,18 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     hs_first = td.hs_slot[th.hs_off + tid];
     hd_first = td.hs_dst[th.hs_off + tid];
   }
-  float* stage = su;  // [te][NC][NPE]
+  float* stage = su;  // [te][NPE][NC]: a slot's components side by side
   const int rs = L.rs;
   if (active) {
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
-      const int base = el * NC * NPE + j * NG + i;
+      const int base = (el * NPE + j * NG + i) * NC;
+      if constexpr (NC == 2) {
+        *reinterpret_cast<float2*>(stage + base) = make_float2(fo[0][j], fo[1][j]);
+      } else {
 #pragma unroll
-      for (int c = 0; c < NC; ++c) stage[base + c * NPE] = fo[c][j];
+        for (int c = 0; c < NC; ++c) stage[base + c] = fo[c][j];
+      }
       const uint32_t rank = (dsc[j] >> kSlotRankShift) & 0xffu;
       if (rank != kSlotRankNone)
         pl[(dsc[j] & kSlotPointMask) * rs + rank] = static_cast<uint16_t>(base | ((dsc[j] & kSlotLast) ? 0x8000 : 0));
@@ -659,7 +669,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
     const int e = ls / NPE, k = ls - e * NPE;
     float val[NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) val[c] = stage[(e * NC + c) * NPE + k];
+    for (int c = 0; c < NC; ++c) val[c] = stage[(e * NPE + k) * NC + c];
     if (dst >= 0) {
 #pragma unroll
       for (int c = 0; c < NC; ++c) td.hbuf[static_cast<size_t>(c) * td.n_hbuf + dst] = val[c];
@@ -701,9 +711,17 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       for (int k = 1; k < 4; ++k) valid[k] = valid[k - 1] && !(e[k - 1] & 0x8000u);
       float x[4][NC];
 #pragma unroll
-      for (int k = 0; k < 4; ++k)
+      for (int k = 0; k < 4; ++k) {
+        const float* sp = stage + (e[k] & 0x7fffu);
+        if constexpr (NC == 2) {
+          const float2 q = valid[k] ? *reinterpret_cast<const float2*>(sp) : make_float2(0.0f, 0.0f);
+          x[k][0] = q.x;
+          x[k][1] = q.y;
+        } else {
 #pragma unroll
-        for (int c = 0; c < NC; ++c) x[k][c] = valid[k] ? stage[(e[k] & 0x7fffu) + c * NPE] : 0.0f;
+          for (int c = 0; c < NC; ++c) x[k][c] = valid[k] ? sp[c] : 0.0f;
+        }
+      }
 #pragma unroll
       for (int k = 0; k < 4; ++k)
 #pragma unroll
@@ -809,7 +827,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ __align__(16) TileSeg s_seg;   // the item's segment, read by the body from shared memory
   __shared__ __align__(16) TileItem s_it;
-  __shared__ int32_t s_idle, s_parity;
+  __shared__ int32_t s_idle;
   static_assert(sizeof(TileSeg) % 4 == 0, "TileSeg is copied as 32-bit words");
   if (threadIdx.x < 20)
     reinterpret_cast<uint32_t*>(&s_it)[threadIdx.x] = reinterpret_cast<const uint32_t*>(items + blockIdx.x)[threadIdx.x];
@@ -819,24 +837,28 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   }
   __syncthreads();
   // this thread's first halo tile point, loaded beside the segment and the state
-  const int32_t g_first = static_cast<int>(threadIdx.x) < s_it.th.ntp - s_it.th.nc ? s_it.halo_tp[threadIdx.x] : -1;
+  const int tg = static_cast<int>(blockDim.x - 1 - threadIdx.x);
+  const int32_t g_first = tg < s_it.th.ntp - s_it.th.nc ? s_it.halo_tp[tg] : -1;
   {
+    // the segment's words; on the solve's odd steps the words of u_cur and
+    // u_nxt are exchanged (both candidates and the parity load together)
+    constexpr int kUc = static_cast<int>((offsetof(TileSeg, td) + offsetof(TiledDev, u_cur)) / 4);
+    constexpr int kUn = static_cast<int>((offsetof(TileSeg, td) + offsetof(TiledDev, u_nxt)) / 4);
+    static_assert(kUn == kUc + 2, "u_cur and u_nxt are adjacent pointers");
     const uint32_t* src = reinterpret_cast<const uint32_t*>(segs + s_it.seg);
     uint32_t* dst = reinterpret_cast<uint32_t*>(&s_seg);
-    for (int q = threadIdx.x; q < static_cast<int>(sizeof(TileSeg) / 4); q += blockDim.x) dst[q] = src[q];
+    for (int q = threadIdx.x; q < static_cast<int>(sizeof(TileSeg) / 4); q += blockDim.x) {
+      if (q >= kUc && q < kUc + 4) {
+        const uint32_t own = src[q], other = src[q < kUn ? q + 2 : q - 2];
+        dst[q] = s_it.st->parity ? other : own;
+      } else {
+        dst[q] = src[q];
+      }
+    }
   }
-  if (threadIdx.x == blockDim.x - 1) {
-    s_idle = s_it.st->mode == kModeIdle;
-    s_parity = s_it.st->parity;
-  }
+  if (threadIdx.x == blockDim.x - 1) s_idle = s_it.st->mode == kModeIdle;
   __syncthreads();
   if (s_idle) return;
-  if (threadIdx.x == 0 && s_parity) {
-    const float* cur = s_seg.td.u_cur;
-    s_seg.td.u_cur = s_seg.td.u_nxt;
-    s_seg.td.u_nxt = const_cast<float*>(cur);
-  }
-  __syncthreads();
   tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial, s_it.tile, &s_it.th, L,
                                   smem_raw, bar, 0u, g_first);
 }
