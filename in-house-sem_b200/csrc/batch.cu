@@ -324,6 +324,7 @@ void Batch::rebuild() {
     d.ngll = c.ngll;
     d.kind = c.kind;
     d.m = c.m;
+    d.ncomp = c.ncomp;
     d.elastic = c.elastic;
     d.segs.upload_async(c.segs, stream);
     d.items.upload_async(c.items, stream);
@@ -347,13 +348,21 @@ void Batch::rebuild() {
     dclasses.push_back(std::move(d));
   }
   {
-    // lanes: classes by work, largest first, each to the least loaded lane
+    // lanes: elastic classes by component count, then the acoustic classes
+    // by work, largest first, each to the least loaded lane
     std::sort(work.begin(), work.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
     std::vector<double> load(n_lanes, 0.0);
     for (const auto& w : work) {
-      const int l = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
-      dclasses[w.second].lane = l;
-      load[l] += w.first;
+      DevClass& d = dclasses[w.second];
+      if (!d.elastic) continue;
+      d.lane = d.ncomp == 3 ? lane3() : 0;
+      load[d.lane] += w.first;
+    }
+    for (const auto& w : work) {
+      DevClass& d = dclasses[w.second];
+      if (d.elastic) continue;
+      d.lane = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+      load[d.lane] += w.first;
     }
   }
   for (int c = 0; c < 3; ++c) {
@@ -418,6 +427,7 @@ void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
   if (tiles_begin) CUDA_CHECK(cudaEventRecord(tiles_begin, stream));
   int used = 1;  // lanes in use: 0 .. used-1
   for (const DevClass& d : dclasses) used = std::max(used, d.lane + 1);
+  if (n_halo_items[2] > 0) used = std::max(used, lane3() + 1);
   if (used > 1) {
     CUDA_CHECK(cudaEventRecord(fork_ev, stream));
     for (int k = 1; k < used; ++k) CUDA_CHECK(cudaStreamWaitEvent(lanes[k - 1], fork_ev, 0));
@@ -438,20 +448,28 @@ void Batch::enqueue(cudaEvent_t tiles_begin, cudaEvent_t tiles_end) {
     a.stream = d.lane == 0 ? stream : lanes[d.lane - 1];
     tile_batch(d.ngll, a, true);
   }
-  for (int k = 1; k < used; ++k) {
-    CUDA_CHECK(cudaEventRecord(join_ev[k - 1], lanes[k - 1]));
-    CUDA_CHECK(cudaStreamWaitEvent(stream, join_ev[k - 1], 0));
+  auto join = [&]() {
+    for (int k = 1; k < used; ++k) {
+      CUDA_CHECK(cudaEventRecord(join_ev[k - 1], lanes[k - 1]));
+      CUDA_CHECK(cudaStreamWaitEvent(stream, join_ev[k - 1], 0));
+    }
+  };
+  // solid halos first: the fluid's coupling term reads the solid's new
+  // acceleration.  Timed runs (tiles_end) keep every tile ahead of the halos.
+  if (tiles_end) {
+    join();
+    CUDA_CHECK(cudaEventRecord(tiles_end, stream));
   }
-  if (tiles_end) CUDA_CHECK(cudaEventRecord(tiles_end, stream));
-  // solid halos first: the fluid's coupling term reads the solid's new acceleration
   if (n_halo_items[1] > 0) {
     halo_batch_kernel<2, true><<<n_halo_items[1], kHaloChunk, 0, stream>>>(dhalo_segs[1].get(), dhalo_items[1].get());
     CUDA_LAUNCH_CHECK();
   }
   if (n_halo_items[2] > 0) {
-    halo_batch_kernel<3, true><<<n_halo_items[2], kHaloChunk, 0, stream>>>(dhalo_segs[2].get(), dhalo_items[2].get());
+    cudaStream_t s3 = tiles_end || lane3() == 0 ? stream : lanes[lane3() - 1];
+    halo_batch_kernel<3, true><<<n_halo_items[2], kHaloChunk, 0, s3>>>(dhalo_segs[2].get(), dhalo_items[2].get());
     CUDA_LAUNCH_CHECK();
   }
+  if (!tiles_end) join();
   if (n_halo_items[0] > 0) {
     halo_batch_kernel<1, false><<<n_halo_items[0], kHaloChunk, 0, stream>>>(dhalo_segs[0].get(), dhalo_items[0].get());
     CUDA_LAUNCH_CHECK();

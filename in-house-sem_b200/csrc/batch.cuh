@@ -104,7 +104,7 @@ class Batch {
   void enqueue(cudaEvent_t tiles_begin = nullptr, cudaEvent_t tiles_end = nullptr);
 
   struct DevClass {
-    int ngll = 0, kind = 0, m = 0;
+    int ngll = 0, kind = 0, m = 0, ncomp = 1;
     bool elastic = false;
     DeviceBuffer<TileSeg> segs;
     DeviceBuffer<TileItem> items;
@@ -121,10 +121,15 @@ class Batch {
   // is `stream`, lane k > 0 is lanes[k - 1]): no tile writes what another
   // tile reads (complete points belong to one tile, halo contributions have
   // their own places), so classes need no order among them.  The lanes fork
-  // after the constrained gathers and join before the halo kernels.  Classes
-  // go to lanes largest first, each to the lane with the least work.
+  // after the constrained gathers.  Elastic classes of two components go to
+  // lane 0 and those of three to lane 1, and each lane then runs the halo
+  // kernel of its component count, which reads only those tiles' output;
+  // acoustic classes go to the least loaded lane.  The lanes join before the
+  // acoustic halo kernel, whose coupling term reads the solid's new
+  // acceleration.
   static constexpr int kMaxLanes = 8;
   int n_lanes = 1;
+  int lane3() const { return n_lanes > 1 ? 1 : 0; }  // the lane of three-component elastic classes
   cudaStream_t lanes[kMaxLanes - 1] = {};
   cudaEvent_t fork_ev = nullptr;
   cudaEvent_t join_ev[kMaxLanes - 1] = {};
