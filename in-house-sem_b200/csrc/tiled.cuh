@@ -821,8 +821,8 @@ static_assert(sizeof(TileItem) == 80, "TileItem is loaded as 20 words");
 // which costs resident CTAs per SM.)  One shared memory layout serves the
 // class (sized for its largest tile).
 template <int NG, int KIND, bool EL, int M>
-static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
-    tile_batch_kernel(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items, TileLayout L) {
+__device__ __forceinline__ void tile_batch_run(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items,
+                                               const TileLayout& L) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ __align__(8) uint64_t bar[2];
   __shared__ __align__(16) TileSeg s_seg;   // the item's segment, read by the body from shared memory
@@ -861,6 +861,21 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   if (s_idle) return;
   tile_step_body<NG, KIND, EL, M>(s_seg.blk, s_seg.td, s_seg.sc, s_seg.st, s_seg.epartial, s_it.tile, &s_it.th, L,
                                   smem_raw, bar, 0u, g_first);
+}
+template <int NG, int KIND, bool EL, int M>
+static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
+    tile_batch_kernel(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items, TileLayout L) {
+  tile_batch_run<NG, KIND, EL, M>(segs, items, L);
+}
+// The same kernel with its registers capped at 96, used for the ngll 7 elastic
+// axisymmetric classes: uncapped they take 99-128 registers, so their CTAs of
+// up to 256 threads fit 2-3 to an SM; capped, their 160-thread tiles fit 4
+// (measured on the 256-model batch: 7.51 -> 7.27 ms per batched step).
+constexpr int kCappedRegs = 96;
+template <int NG, int KIND, bool EL, int M>
+static __global__ void __maxnreg__(kCappedRegs)
+    tile_batch_kernel_capped(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items, TileLayout L) {
+  tile_batch_run<NG, KIND, EL, M>(segs, items, L);
 }
 
 // ------------------------------------------------------------ halo kernel

@@ -136,6 +136,10 @@ int tile_batch_cfg(const TileBatchLaunch& a, bool launch) {
     return 0;
   };
   if (a.kind == INSEM_AXISYM) {
+    if constexpr (NG == 7) {
+      if (a.elastic) return a.m == 1 ? go(tile_batch_kernel_capped<NG, INSEM_AXISYM, true, 1>)
+                                     : go(tile_batch_kernel_capped<NG, INSEM_AXISYM, true, 0>);
+    }
     if (a.m == 1) return a.elastic ? go(tile_batch_kernel<NG, INSEM_AXISYM, true, 1>)
                                    : go(tile_batch_kernel<NG, INSEM_AXISYM, false, 1>);
     return a.elastic ? go(tile_batch_kernel<NG, INSEM_AXISYM, true, 0>) : go(tile_batch_kernel<NG, INSEM_AXISYM, false, 0>);
