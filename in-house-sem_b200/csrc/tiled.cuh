@@ -538,12 +538,19 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
         float uxi[NC], ueta[NC];
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
+          // the row two entries per 8-byte load (rows are ROW = even floats
+          // long and start on 8-byte boundaries; the pad entry is never used)
           const float* row = urow + ridx(c, j, 0);
           float a = 0.0f, b = 0.0f;
 #pragma unroll
-          for (int l = 0; l < NG; ++l) {
-            a = fadd(a, fmul(dxr[l], row[l]));
+          for (int l = 0; l < NG; l += 2) {
+            const float2 r2 = *reinterpret_cast<const float2*>(row + l);
+            a = fadd(a, fmul(dxr[l], r2.x));
             b = fadd(b, fmul(cbasis(NG, 0, j * NG + l), ucol[c][l]));
+            if (l + 1 < NG) {
+              a = fadd(a, fmul(dxr[l + 1], r2.y));
+              b = fadd(b, fmul(cbasis(NG, 0, j * NG + l + 1), ucol[c][l + 1]));
+            }
           }
           uxi[c] = a;
           ueta[c] = b;
@@ -616,9 +623,14 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
           const float* row = frow + ridx(c, j, 0);
           float acc = 0.0f;
 #pragma unroll
-          for (int l = 0; l < NG; ++l) {
-            acc = fadd(acc, fmul(dxc[l], row[l]));
+          for (int l = 0; l < NG; l += 2) {
+            const float2 r2 = *reinterpret_cast<const float2*>(row + l);
+            acc = fadd(acc, fmul(dxc[l], r2.x));
             acc = fadd(acc, fmul(cbasis(NG, 0, l * NG + j), fe[c][l]));
+            if (l + 1 < NG) {
+              acc = fadd(acc, fmul(dxc[l + 1], r2.y));
+              acc = fadd(acc, fmul(cbasis(NG, 0, (l + 1) * NG + j), fe[c][l + 1]));
+            }
           }
           s[c] = acc;
         }
