@@ -879,13 +879,16 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
     tile_batch_kernel(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items, TileLayout L) {
   tile_batch_run<NG, KIND, EL, M>(segs, items, L);
 }
-// The same kernel with its registers capped at 96, used for the ngll 7 elastic
-// axisymmetric classes: uncapped they take 99-128 registers, so their CTAs of
-// up to 256 threads fit 2-3 to an SM; capped, their 160-thread tiles fit 4
-// (measured on the 256-model batch: 7.51 -> 7.27 ms per batched step).
-constexpr int kCappedRegs = 96;
-template <int NG, int KIND, bool EL, int M>
-static __global__ void __maxnreg__(kCappedRegs)
+// Register budgets for the elastic axisymmetric batch classes whose CTAs
+// per SM shared memory or the launch's thread count limit anyway: the
+// budget is what those CTAs can use.  Uncapped, the compiler gives the ngll
+// 7 kernels 99-128 registers (2-3 CTAs per SM where 4 fit) and the ngll 5
+// and 6 m=1 kernels 80 with 44-60 bytes of spills although their shared
+// memory allows only 3 CTAs.  0: no cap (the kernel's launch bounds apply).
+template <int NG, int M>
+constexpr int kBatchRegs = NG == 7 ? (M == 1 ? 112 : 96) : (M == 1 ? (NG == 6 ? 104 : NG == 5 ? 96 : 0) : 0);
+template <int NG, int KIND, bool EL, int M, int REGS>
+static __global__ void __maxnreg__(REGS)
     tile_batch_kernel_capped(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items, TileLayout L) {
   tile_batch_run<NG, KIND, EL, M>(segs, items, L);
 }

@@ -136,9 +136,11 @@ int tile_batch_cfg(const TileBatchLaunch& a, bool launch) {
     return 0;
   };
   if (a.kind == INSEM_AXISYM) {
-    if constexpr (NG == 7) {
-      if (a.elastic) return a.m == 1 ? go(tile_batch_kernel_capped<NG, INSEM_AXISYM, true, 1>)
-                                     : go(tile_batch_kernel_capped<NG, INSEM_AXISYM, true, 0>);
+    if (a.elastic) {
+      if constexpr (kBatchRegs<NG, 1> > 0)
+        if (a.m == 1) return go(tile_batch_kernel_capped<NG, INSEM_AXISYM, true, 1, kBatchRegs<NG, 1>>);
+      if constexpr (kBatchRegs<NG, 0> > 0)
+        if (a.m == 0) return go(tile_batch_kernel_capped<NG, INSEM_AXISYM, true, 0, kBatchRegs<NG, 0>>);
     }
     if (a.m == 1) return a.elastic ? go(tile_batch_kernel<NG, INSEM_AXISYM, true, 1>)
                                    : go(tile_batch_kernel<NG, INSEM_AXISYM, false, 1>);
