@@ -788,9 +788,9 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
 }
 
 template <int NG, int KIND, bool EL, int M>
-static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
-    tile_step_kernel(BlockDev blk, TiledDev td, StepScalars sc, StepState* __restrict__ st,
-                     double* __restrict__ epartial, int32_t tile0, TileLayout L) {
+__device__ __forceinline__ void tile_step_run(const BlockDev& blk, const TiledDev& td, const StepScalars& sc,
+                                              StepState* __restrict__ st, double* __restrict__ epartial,
+                                              int32_t tile0, const TileLayout& L) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem_raw + L.bar);
   if (threadIdx.x == 0) {
@@ -800,6 +800,12 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
   __syncthreads();
   const int32_t tile = tile0 + blockIdx.x;
   tile_step_body<NG, KIND, EL, M>(blk, td, sc, st, epartial, tile, td.tiles + tile, L, smem_raw, bar, 0u);
+}
+template <int NG, int KIND, bool EL, int M>
+static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
+    tile_step_kernel(BlockDev blk, TiledDev td, StepScalars sc, StepState* __restrict__ st,
+                     double* __restrict__ epartial, int32_t tile0, TileLayout L) {
+  tile_step_run<NG, KIND, EL, M>(blk, td, sc, st, epartial, tile0, L);
 }
 
 // Tiles of many solves in one launch.  A segment is one block of one
@@ -886,7 +892,7 @@ static __global__ void __launch_bounds__(TileCfg<NG>::THREADS)
 // and 6 m=1 kernels 80 with 44-60 bytes of spills although their shared
 // memory allows only 3 CTAs.  0: no cap (the kernel's launch bounds apply).
 template <int NG, int M>
-constexpr int kBatchRegs = NG == 7 ? (M == 1 ? 112 : 96) : (M == 1 ? (NG == 6 ? 104 : NG == 5 ? 96 : 0) : 0);
+constexpr int kBatchRegs = NG == 7 ? (M == 1 ? 128 : 96) : (M == 1 ? (NG == 6 ? 112 : NG == 5 ? 96 : 0) : 0);
 template <int NG, int KIND, bool EL, int M, int REGS>
 static __global__ void __maxnreg__(REGS)
     tile_batch_kernel_capped(const TileSeg* __restrict__ segs, const TileItem* __restrict__ items, TileLayout L) {

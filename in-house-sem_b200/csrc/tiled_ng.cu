@@ -31,6 +31,10 @@ void INSEM_CAT(set_constant_basis_ng, INSEM_NG)(const float* D, const float* Dj,
 
 int INSEM_CAT(tile_elements_ng, INSEM_NG)() { return TileCfg<INSEM_NG>::TE; }
 
+int INSEM_CAT(tile_step_occupancy_ng, INSEM_NG)(int kind, bool elastic, int m, int te, uint32_t smem) {
+  return tile_step_occupancy_cfg<INSEM_NG>(kind, elastic, m, te, smem);
+}
+
 int INSEM_CAT(tile_batch_ng, INSEM_NG)(const TileBatchLaunch& a, bool launch) {
   return tile_batch_cfg<INSEM_NG>(a, launch);
 }

@@ -137,7 +137,35 @@ void set_tile_elements(int ngll, int kind, bool elastic, int m, int te) {
   else g_tile_table[tile_key(ngll, kind, elastic, m)] = te;
 }
 
+int tile_step_occupancy(int ngll, int kind, bool elastic, int m, int te, uint32_t smem) {
+  switch (ngll) {
+    case 2: return tile_step_occupancy_ng2(kind, elastic, m, te, smem);
+    case 3: return tile_step_occupancy_ng3(kind, elastic, m, te, smem);
+    case 4: return tile_step_occupancy_ng4(kind, elastic, m, te, smem);
+    case 5: return tile_step_occupancy_ng5(kind, elastic, m, te, smem);
+    case 6: return tile_step_occupancy_ng6(kind, elastic, m, te, smem);
+    case 7: return tile_step_occupancy_ng7(kind, elastic, m, te, smem);
+    case 8: return tile_step_occupancy_ng8(kind, elastic, m, te, smem);
+    case 9: return tile_step_occupancy_ng9(kind, elastic, m, te, smem);
+    default: return -1;
+  }
+}
+
 int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp) {
+  // one answer per class and device (the occupancy queries below ask the device)
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int> cache;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    dev = -1;
+  }
+  const int key = ((((ngll * 4 + kind) * 2 + (elastic ? 1 : 0)) * 2 + m) * 4 + ncomp);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    const auto it = cache.find({dev, key});
+    if (it != cache.end()) return it->second;
+  }
   const int te_max = tile_elements(ngll);
   const int q = ngll - 1;
   double best = -1.0;
@@ -149,7 +177,12 @@ int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp) {
     const int nc = te * q * q;
     const int tp = nc + 4 * side * q + 4;
     const TileLayout L = TileLayout::make(ngll, ncomp, kind, elastic, te, (tp + 3) & ~3, (nc + 3) & ~3, 4);
-    const int ctas = std::min({(228 * 1024) / (static_cast<int>(L.total) + 1024), 2048 / tile_threads(te, ngll), 32});
+    // CTAs per SM: the device's answer for the kernel (its registers count
+    // too), else shared memory alone with 2 KB per CTA for the reserved and
+    // static parts
+    const int occ = dev >= 0 ? tile_step_occupancy(ngll, kind, elastic, m, te, L.total) : -1;
+    const int by_smem = (228 * 1024) / (static_cast<int>(L.total) + 2048);
+    const int ctas = std::min({occ >= 0 ? occ : by_smem, 2048 / tile_threads(te, ngll), 32});
     if (ctas < 1) continue;
     const double halo = static_cast<double>(tp - nc) / tp;                 // points shared with other tiles
     const double overlap = ctas >= 3 ? 1.0 : ctas == 2 ? 0.9 : 0.6;       // copies of one tile under another's math
@@ -160,7 +193,10 @@ int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp) {
       best_te = te;
     }
   }
-  (void)m;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    cache[{dev, key}] = best_te;
+  }
   return best_te;
 }
 

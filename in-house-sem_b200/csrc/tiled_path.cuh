@@ -87,6 +87,46 @@ int tile_elements(int ngll);  // TileCfg<NG>::TE (the largest tile)
 int choose_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp, int requested);
 void set_tile_elements(int ngll, int kind, bool elastic, int m, int te);  // te <= 0 clears the entry
 int analytic_tile_elements(int ngll, int kind, bool elastic, int m, int ncomp);
+// CTAs per SM of the plain tile kernel of a class at te elements and smem
+// bytes of dynamic shared memory (registers, shared memory and threads as
+// the current device counts them); -1 if the device cannot be asked.
+int tile_step_occupancy(int ngll, int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng2(int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng3(int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng4(int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng5(int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng6(int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng7(int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng8(int kind, bool elastic, int m, int te, uint32_t smem);
+int tile_step_occupancy_ng9(int kind, bool elastic, int m, int te, uint32_t smem);
+
+template <int NG>
+int tile_step_occupancy_cfg(int kind, bool elastic, int m, int te, uint32_t smem) {
+  auto ask = [&](auto kernel) -> int {
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, tile_threads(te, NG), smem) != cudaSuccess) {
+      cudaGetLastError();
+      return -1;
+    }
+    return nb;
+  };
+  if (kind == INSEM_AXISYM) {
+    if (m == 1) return elastic ? ask(tile_step_kernel<NG, INSEM_AXISYM, true, 1>) : ask(tile_step_kernel<NG, INSEM_AXISYM, false, 1>);
+    return elastic ? ask(tile_step_kernel<NG, INSEM_AXISYM, true, 0>) : ask(tile_step_kernel<NG, INSEM_AXISYM, false, 0>);
+  }
+  switch (kind) {
+    case INSEM_RECT:
+      return elastic ? ask(tile_step_kernel<NG, INSEM_RECT, true, 0>) : ask(tile_step_kernel<NG, INSEM_RECT, false, 0>);
+    case INSEM_AFFINE:
+      return elastic ? ask(tile_step_kernel<NG, INSEM_AFFINE, true, 0>) : ask(tile_step_kernel<NG, INSEM_AFFINE, false, 0>);
+    default:
+      return elastic ? ask(tile_step_kernel<NG, INSEM_CURVED, true, 0>) : ask(tile_step_kernel<NG, INSEM_CURVED, false, 0>);
+  }
+}
 // Uploads the GLL / GLJ basis of one ngll to constant memory (must agree with earlier uploads).
 void set_constant_basis(int ngll, const std::vector<float>& D, const std::vector<float>& Dj,
                         const std::vector<float>& w2);
