@@ -1074,8 +1074,14 @@ __device__ __forceinline__ void halo_step_body(const TiledDev& td, const HaloDev
   }
 }
 
+// Register budgets of the halo kernels (256 threads per CTA): two-component
+// points fit in 48 registers without spills (5 CTAs per SM instead of 4);
+// three-component ones in 64 with 40 bytes of spills in the rarely taken
+// Stacey solve (4 CTAs instead of 3).
+template <int NC>
+constexpr int kHaloRegs = NC == 2 ? 48 : 64;
 template <int NC, bool ELASTIC>
-static __global__ void __launch_bounds__(256)
+static __global__ void __maxnreg__(kHaloRegs<NC>)
     halo_step_kernel(TiledDev td, HaloDev hd, CouplingDev cp, const float* __restrict__ other, int32_t other_ng,
                      bool pm, const float* __restrict__ amp, int32_t n_amp, StepScalars sc, double h_damp,
                      const StepState* __restrict__ st, double* __restrict__ epartial, int32_t epart0) {
@@ -1160,7 +1166,7 @@ struct HaloSeg {
 };
 
 template <int NC, bool ELASTIC>
-static __global__ void __launch_bounds__(kHaloChunk) halo_batch_kernel(const HaloSeg* __restrict__ segs,
+static __global__ void __maxnreg__(kHaloRegs<NC>) halo_batch_kernel(const HaloSeg* __restrict__ segs,
                                                                          const int2* __restrict__ items) {
   const int2 it = items[blockIdx.x];
   const HaloSeg& sg = segs[it.x];
