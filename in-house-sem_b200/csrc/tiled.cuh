@@ -27,6 +27,7 @@
 
 #include <cstddef>
 
+
 #include "element_ops.cuh"
 #include "step_kernels.cuh"
 
@@ -208,6 +209,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 }
 constexpr uint32_t kBulkWaitLimit = 1u << 22;
 
+// Whether a class writes its f_xi rows as the fluxes are formed (into a
+// region of their own, fewer registers held across the barrier) instead of
+// after the barrier into the dead element data (less shared memory).  Only
+// three-component classes, and of the benchmarked orders only ngll 6, gain
+// from it under their register budgets (256-model batch, per class: ngll 6
+// m=1 0.147 vs 0.154 ms early vs late; ngll 5 0.106 vs 0.103; ngll 7 0.229
+// vs 0.224).
+__host__ __device__ constexpr bool early_flux_rows(int ng, int nc) { return nc == 3 && ng != 5 && ng != 7; }
+
 // Shared-memory layout of one tile CTA, byte offsets (16-byte aligned).
 // Per-tile data arrives by bulk copies: element data (metric, axisymmetric
 // weights), slot descriptors, and the complete points' u, v and inverse mass
@@ -260,10 +270,10 @@ struct TileLayout {
     // su doubles as the halo staging area: [te][nc][npe]
     o = up16(o + 4u * te * (rows > static_cast<uint32_t>(nc * npe) ? rows : static_cast<uint32_t>(nc * npe)));
     const uint32_t sfx_b = up16(4u * te * rows);
-    // three-component classes write their f_xi rows as the fluxes are formed
-    // (fewer registers held across the barrier), so their rows cannot sit in
-    // the element data the fluxes still read
-    if (sfx_b <= elem && nc != 3) {
+    // classes that write their f_xi rows as the fluxes are formed
+    // (early_flux_rows) cannot keep them in the element data the fluxes
+    // still read
+    if (sfx_b <= elem && !early_flux_rows(ng, nc)) {
       L.sfx = L.metric;
     } else {
       L.sfx = o;
@@ -562,7 +572,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
                                     ax + 3 * AXS, w2c[j], ec0, ec1);
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          if constexpr (NC == 3) frow[ridx(c, j, i)] = fxp[c];  // own region: store now
+          if constexpr (early_flux_rows(NG, NC)) frow[ridx(c, j, i)] = fxp[c];  // own region: store now
           else fx[c][j] = fxp[c];
           fe[c][j] = fy[c];
         }
@@ -584,7 +594,7 @@ __device__ __forceinline__ bool tile_step_body(const BlockDev& blk, const TiledD
       bulk_load(s_im, td.inv_mass + th.cbeg, 4u * nc4, bar + 1);
     }
   }
-  if (active && NC != 3) {
+  if (active && !early_flux_rows(NG, NC)) {
 #pragma unroll
     for (int j = 0; j < NG; ++j) {
       if constexpr (PAIR) {

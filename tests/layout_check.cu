@@ -88,7 +88,7 @@ int main() {
             const Region ax{"axis terms", L.ax, L.ax + (kind == 3 ? 4u * te * 4 * ((ng + 3) & ~3) : 0u)};
             // phases 1-3a: copies land, rows are built, fluxes read the element data
             std::vector<Region> p1 = {bar, elem, u, su, ax};
-            if (nc == 3) p1.push_back(sfx);  // three-component classes write their f_xi rows during the fluxes
+            if (insem_b200::early_flux_rows(ng, nc)) p1.push_back(sfx);  // f_xi rows written during the fluxes
             // phases 3b-4: flux rows written and read; the element data is dead, and
             // v and 1/M arrive (late copies) or are held
             std::vector<Region> p2 = {bar, u, su, ax, sfx, v, im};
